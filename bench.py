@@ -1,0 +1,388 @@
+"""Benchmark: population fitness evaluation, node-evals/s on B200.
+
+One step = one generation's evaluation of the whole batched population (10,000
+expressions of 3-63 tokens, 5 variables, 1M datapoints): every expression on
+every datapoint, reduced to per-expression MSE, through the persistent
+interpreter kernel plus the span-combine kernel.  A node-eval is one token of
+an original expression evaluated at one datapoint.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU; every rank evaluates its own
+seeded shard of the population (weak scaling, no collective on the data path).
+`--impl reference` times the reference's own CPU evaluator (evaluate_cpu_mse,
+compiled unchanged into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-evals/s fwd and fwd+adjoint at <=1e-5 rel err vs FP64 oracle, 1 B200"
+UNIT = "node-evals/s"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "plain", "cache", "grad", "large"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="target CPU work of the CPU-baseline sample")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-baseline", action="store_true",
+                    help="also time the plain per-expression kernel")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def make_workload(name: str, rank: int):
+    from symbolic_regression_gpu_b200 import synth
+    fn = synth.WORKLOADS[name]
+    seeds = {"plain": 1, "batched": 2, "cache": 3, "grad": 4, "large": 5}
+    return fn(seed=seeds[name] + 1000 * rank)
+
+
+def config_of(w, world: int, flush: str):
+    return {"workload": w.name, "exprs_per_gpu": w.population.num_exprs,
+            "global_exprs": w.population.num_exprs * world,
+            "tokens_per_gpu": int(w.population.num_tokens),
+            "mean_len": round(float(w.meta["len_mean"]), 2), "num_vars": w.num_vars,
+            "num_dps": w.num_dps, "x_range": w.meta.get("x_range"),
+            "ops": "+ - * loose_div sin cos exp_clamp80 loose_log loose_sqrt",
+            "parallelism": f"expr-shard x{world}" if world > 1 else "single",
+            "l2": flush}
+
+
+# ---- clocks -------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_uuid=None):
+        self.proc = None
+        self.out = os.path.join("/tmp", f"sr_clocks_{os.getpid()}.csv")
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if device_uuid:
+            cmd += ["-i", device_uuid]
+        try:
+            self.fh = open(self.out, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.out) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.out)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---- CPU baseline ---------------------------------------------------------------
+
+def _reference_population(pop):
+    """The reference evaluator has no exp-clamp opcode: map it to its EXP
+    (same expf call) for timing."""
+    from symbolic_regression_gpu_b200.population import Population
+    tok = pop.tokens.copy()
+    tok[tok == 32] = 16
+    return Population(tok, pop.values, pop.offsets)
+
+
+def cpu_baseline(w, target_s: float, threads: int):
+    """Reference evaluate_cpu_mse (oracle/_ref, compiled -O3) on a seeded
+    expression subset over the full datapoint range."""
+    from oracle import oracle
+    pop = _reference_population(w.population)
+    E = pop.num_exprs
+    rng = np.random.default_rng(7)
+    order = rng.permutation(E)
+    # Probe the rate, then size the sample to ~target_s of CPU work.
+    n_probe = max(threads, min(E, 16))
+    probe = pop.subset(order[:n_probe])
+    t0 = time.perf_counter()
+    oracle.ref_mse(probe, w.X, threads=threads)
+    rate = probe.num_tokens * w.num_dps / max(time.perf_counter() - t0, 1e-6)
+    tokens_target = rate * target_s / w.num_dps
+    mean_len = pop.num_tokens / E
+    n = int(max(threads, min(E, tokens_target / mean_len)))
+    sample = pop.subset(order[:n])
+    t0 = time.perf_counter()
+    oracle.ref_mse(sample, w.X, threads=threads)
+    dt = time.perf_counter() - t0
+    value = sample.num_tokens * w.num_dps / dt
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n} of {E} expressions (seeded subset) x all {w.num_dps} datapoints, "
+                      f"{dt:.1f} s; reference evaluate_cpu_mse (src/cleaned/cl_cpu_eval.cpp) "
+                      f"compiled -O3, THREADS={threads}; exp_clamp80 timed as the reference "
+                      f"EXP opcode"}
+
+
+# ---- reference arm ------------------------------------------------------------------
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libref_oracle.so was not built"}))
+        return 0
+    w = make_workload(args.workload, 0)
+    threads = os.cpu_count() or 1
+    pop = _reference_population(w.population)
+    E = pop.num_exprs
+    rng = np.random.default_rng(7)
+    order = rng.permutation(E)
+    # Size one step's sample so warmup+steps stay within a few minutes.
+    probe = pop.subset(order[:max(threads, 16)])
+    t0 = time.perf_counter()
+    oracle.ref_mse(probe, w.X, threads=threads)
+    rate = probe.num_tokens * w.num_dps / max(time.perf_counter() - t0, 1e-6)
+    per_step_s = min(20.0, 150.0 / max(args.steps + args.warmup, 1))
+    n = int(max(threads, min(E, rate * per_step_s / w.num_dps / (pop.num_tokens / E))))
+    sample = pop.subset(order[:n])
+    for _ in range(args.warmup):
+        oracle.ref_mse(sample, w.X, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.ref_mse(sample, w.X, threads=threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample.num_tokens * w.num_dps * len(times) / total
+    desc = (f"{n} of {E} expressions (seeded subset) x all {w.num_dps} datapoints per step; "
+            f"reference evaluate_cpu_mse compiled -O3, THREADS={threads}; exp_clamp80 timed "
+            f"as the reference EXP opcode")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; stands in for AI-Feynman)",
+            "config": config_of(w, 1, "n/a (CPU)"), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                             "kind": "reference", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our arm ----------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    from symbolic_regression_gpu_b200 import Evaluator
+
+    w = make_workload(args.workload, rank)
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    tune_path = os.path.join("/tmp", f"sr_tune_{os.getuid()}.json")
+    ev = Evaluator(device=local_rank, autotune=True, tune_cache_path=tune_path)
+    sr_stream = torch.cuda.ExternalStream(ev.stream_handle, device=dev)
+    ev.set_data(w.X)
+    ev.prepare(w.population)  # compile + upload + shape tuning (outside timing)
+    node_evals = w.population.num_tokens * w.num_dps
+
+    def step():
+        with torch.cuda.stream(sr_stream):
+            flush_buf.fill_(1.0)  # evict the dataset from L2 between steps
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(sr_stream)
+        ev.launch()
+        e.record(sr_stream)
+        e.synchronize()
+        launch_ms, kern_ms = ev.last_launch_times()
+        return s.elapsed_time(e), kern_ms
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    mse = ev.read_mse()
+    st = ev.stats
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        uuid = None
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(uuid)
+    step_ms, kern_ms = [], []
+    for _ in range(args.steps):
+        a, b = step()
+        step_ms.append(a)
+        kern_ms.append(b)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = node_evals * world * len(step_ms) / (total_ms * 1e-3)
+    mean_kern_ms = sum(kern_ms) / len(kern_ms)
+
+    # Roofline of the interpreter kernel: declared FP32/SFU work per launch
+    # against the measured pipe peaks of this device.
+    fp32_peak, sfu_peak, nsm = ev.measure_pipes()
+    t_fp32 = st.declared_fp32_ops / fp32_peak
+    t_sfu = st.declared_sfu_ops / sfu_peak
+    bound = "sfu" if t_sfu >= t_fp32 else "fp32"
+    ops = st.declared_sfu_ops if bound == "sfu" else st.declared_fp32_ops
+    peak = sfu_peak if bound == "sfu" else fp32_peak
+    achieved = ops / (mean_kern_ms * 1e-3)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"interp_{args.workload}_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+
+    # Plain per-expression kernel on the same population (baseline ratio).
+    plain = None
+    if args.plain_baseline and rank == 0:
+        ev.prepare(w.population, plain=True)
+        ev.launch()
+        ev.read_mse()
+        pm = []
+        for _ in range(2):
+            a, _ = step()
+            pm.append(a)
+        plain = {"value": node_evals / (statistics.mean(pm) * 1e-3), "unit": UNIT,
+                 "ms_per_step": statistics.mean(pm)}
+        ev.prepare(w.population)
+
+    # End to end through the public API: pinned host dataset and host
+    # population in, MSE vector out, every step.
+    Xp = torch.empty(w.X.shape, dtype=torch.float32, pin_memory=True)
+    Xp.numpy()[...] = w.X
+    e2e_times, h2d, d2h = [], 0, 0
+    for k in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev.set_data(Xp.numpy())
+        out = ev.eval_mse(w.population)
+        dt = time.perf_counter() - t0
+        if k > 0:
+            e2e_times.append(dt)
+        h2d = int(Xp.numel() * 4 + ev.stats.h2d_bytes)
+        d2h = int(ev.stats.d2h_bytes)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = node_evals * world / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(w, args.cpu_seconds, os.cpu_count() or 1)
+        except (ImportError, FileNotFoundError, OSError) as ex:
+            cpu = {"value": None, "unavailable": str(ex)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": len(step_ms), "warmup": max(args.warmup, 3),
+            "ms_per_step": total_ms / len(step_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; stands in for AI-Feynman)",
+            "config": config_of(w, world, "flushed between steps (256 MiB write)"),
+            "mode": "fwd",
+            "kernel": {"dpt": st.dpt, "warps_per_block": st.warps_per_block,
+                       "blocks": st.blocks, "work_items": st.work_items,
+                       "interp_ms_mean": mean_kern_ms},
+            "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "op/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "measured on this GPU by sr_measure_pipes "
+                                        f"({'MUFU rsqrt' if bound == 'sfu' else 'FP32 FMA'} "
+                                        f"microbenchmark, {nsm} SMs)",
+                         "model": "declared per-operator FP32/SFU counts (T_min = "
+                                  "max(F/P_fp32, S/P_sfu))",
+                         "fp32_frac": (st.declared_fp32_ops / (mean_kern_ms * 1e-3)) / fp32_peak,
+                         "sfu_frac": (st.declared_sfu_ops / (mean_kern_ms * 1e-3)) / sfu_peak},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": int(st.kernel_launches) * len(step_ms),
+            "clocks": clk,
+            "plain_kernel": plain,
+            "mse_finite": int(np.isfinite(mse).sum()),
+        }
+        print(json.dumps(line))
+    ev.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,299 @@
+/*
+ * sr_eval.h — C ABI of the B200 population evaluator.
+ *
+ * The hot path is fitness evaluation of a whole GP population: every
+ * prefix-encoded expression is evaluated on every datapoint of one shared
+ * dataset and reduced to its mean squared error.  In the reference
+ * (phi-jkim/symbolic_regression_gpu) this is evaluate_gpu_mse_wrapper
+ * (src/cleaned/cl_gpu_eval.cu:578-592), evaluate_gpu_simple_wrapper
+ * (src/cleaned/cl_gpu_simple.cu:324-336) and the CPU evaluator
+ * evaluate_cpu_mse (src/cleaned/cl_cpu_eval.cpp:94-168).  Those are C++
+ * functions taking InputInfo& / std::vector<float>&; the same entry points
+ * with their exact C++ signatures are exported by this library too (see
+ * sr_reference_abi.h).  This header is the language-neutral boundary: plain
+ * pointers and sizes, status codes instead of exit(), no C++ or torch types.
+ *
+ * Token encoding (reference src/utils/opcodes.h:10-40): a population is a
+ * set of prefix token arrays.  Token 0 = constant (value = the constant),
+ * token -1 = variable (value = variable index as a number), tokens 1..9 are
+ * binary operators, 10..27 unary operators.  Expressions are evaluated right
+ * to left with a stack; for a binary operator the first value popped is the
+ * LEFT operand (reference cl_gpu_eval.cu:98-101).  Token 32 is an extension
+ * of this library (exp with its argument clamped at 80); the reference has no
+ * such opcode.
+ *
+ * Data layout: X is column-major, X[v * num_dps + dp] for v in [0, num_vars],
+ * with the target y in row num_vars (reference flatten_X_col_major_full,
+ * cl_gpu_eval.cu:249-257).
+ *
+ * Threading: a context is used from one host thread at a time.  Every
+ * sr_eval_* call is synchronous: results are valid on return.
+ */
+#ifndef SR_EVAL_H
+#define SR_EVAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SR_ABI_VERSION 1
+
+/* ---- token encoding (reference src/utils/opcodes.h:10-40) ---------------- */
+#define SR_TOK_CONST 0
+#define SR_TOK_VAR (-1)
+#define SR_OP_ADD 1
+#define SR_OP_SUB 2
+#define SR_OP_MUL 3
+#define SR_OP_DIV 4
+#define SR_OP_POW 5
+#define SR_OP_MIN 6
+#define SR_OP_MAX 7
+#define SR_OP_LOOSE_DIV 8
+#define SR_OP_LOOSE_POW 9
+#define SR_OP_SIN 10
+#define SR_OP_COS 11
+#define SR_OP_TAN 12
+#define SR_OP_SINH 13
+#define SR_OP_COSH 14
+#define SR_OP_TANH 15
+#define SR_OP_EXP 16
+#define SR_OP_LOG 17
+#define SR_OP_INV 18
+#define SR_OP_ASIN 19
+#define SR_OP_ACOS 20
+#define SR_OP_ATAN 21
+#define SR_OP_LOOSE_LOG 22
+#define SR_OP_LOOSE_INV 23
+#define SR_OP_ABS 24
+#define SR_OP_NEG 25
+#define SR_OP_SQRT 26
+#define SR_OP_LOOSE_SQRT 27
+/* Extension (no reference counterpart): expf(fminf(x, 80.0f)). */
+#define SR_OP_EXP_CLAMP 32
+
+/* Longest expression accepted (tokens).  The reference caps generated
+ * expressions at MAX_TOKEN_NUM = 64 (src/utils/utils.h:20); this library
+ * accepts longer ones. */
+#define SR_MAX_TOKENS 1024
+/* Largest number of input variables (reference MAX_NUM_FEATURES = 32 incl. y,
+ * src/cleaned/cl_gpu_common.h:9-11). */
+#define SR_MAX_VARS 31
+
+typedef enum sr_status {
+  SR_OK = 0,
+  SR_ERR_INVALID_ARGUMENT = 1,   /* null pointer, negative size, ...          */
+  SR_ERR_BAD_TOKEN = 2,          /* token outside the encoding above          */
+  SR_ERR_MALFORMED_EXPRESSION = 3, /* stack underflow or != 1 result value    */
+  SR_ERR_EXPRESSION_TOO_LONG = 4,  /* more than SR_MAX_TOKENS tokens          */
+  SR_ERR_NO_DATA = 5,            /* no dataset resident on the device          */
+  SR_ERR_CUDA = 6,               /* a CUDA runtime call failed                 */
+  SR_ERR_OUT_OF_MEMORY = 7,      /* device or pinned host allocation failed    */
+  SR_ERR_DEVICE_TIMEOUT = 8,     /* a bounded device-side wait gave up         */
+  SR_ERR_DEVICE_CHECK = 9,       /* a device-side bounds check fired           */
+  SR_ERR_UNSUPPORTED = 10,       /* option or size this build does not handle  */
+  SR_ERR_NO_DEVICE = 11,         /* no CUDA device / extension unusable        */
+  SR_ERR_TOO_MANY_VARS = 12      /* num_vars > SR_MAX_VARS                     */
+} sr_status;
+
+/* Evaluation flags. */
+#define SR_EVAL_SUBTREE_CACHE 0x1u /* use the cross-generation subtree cache  */
+#define SR_EVAL_CLEAR_CACHE 0x2u   /* drop the cache first (reference clear_cache) */
+#define SR_EVAL_PLAIN 0x4u         /* plain per-expression kernel (baseline)   */
+
+typedef struct sr_context sr_context;
+
+typedef struct sr_options {
+  int32_t device;           /* CUDA device ordinal; -1 = the current device   */
+  int32_t cache_capacity;   /* subtree-cache slots; reference: 2048
+                               (MAX_CACHED_SUBTREES, cl_gpu_common.h:13)       */
+  int32_t min_subtree_size; /* detection min size; reference 3 (cl_gpu_eval.cu:373) */
+  int32_t min_subtree_freq; /* detection min frequency; reference 10 (same line) */
+  int32_t dpt;              /* datapoints per thread: 0 = tuned, 4 or 8        */
+  int32_t warps_per_block;  /* evaluating warps per block: 0 = tuned, 1..8     */
+  int32_t autotune;         /* 1 = time candidate launch shapes on first use  */
+  int32_t use_graphs;       /* 1 = replay each launch shape from a CUDA graph */
+  int32_t host_threads;     /* host compile threads; 0 = hardware concurrency  */
+  int32_t reserved0;
+  const char *tune_cache_path; /* JSON file for tuned shapes; NULL = none      */
+  void *stream;             /* cudaStream_t to run on; NULL = own stream      */
+} sr_options;
+
+/* A population in CSR form: expression i is tokens/values[offsets[i] ..
+ * offsets[i+1]).  values are doubles as in the reference InputInfo.values
+ * (src/utils/utils.h:31); constants are used as (float)value and variable
+ * indices as (int)value, exactly as the reference evaluators do. */
+typedef struct sr_population {
+  int32_t num_exprs;
+  int32_t reserved0;
+  const int32_t *tokens;
+  const double *values;
+  const int64_t *offsets; /* num_exprs + 1 entries, offsets[0] == 0 */
+} sr_population;
+
+/* Per-call statistics; the first block mirrors the reference RunStats
+ * (src/utils/utils.h:103-114). */
+typedef struct sr_stats {
+  double total_eval_time_ms;    /* wall time of the call                       */
+  double detect_time_ms;        /* host subtree detection (RunStats.drift_detect_time_ms) */
+  double data_transfer_time_ms; /* host<->device copies (device-timed)        */
+  double gpu_kernel_time_ms;    /* all kernels of the call (device-timed)     */
+  int32_t num_subtrees;         /* common subtrees detected this call         */
+  int32_t new_subtrees;         /* of which newly evaluated into the cache    */
+  double avg_subtree_size;
+  double coverage;              /* covered tokens / total tokens (detection)  */
+  /* additions */
+  double host_compile_time_ms;  /* token validation + bytecode compilation    */
+  double eval_kernel_time_ms;   /* main interpreter kernel only               */
+  int64_t node_evals;           /* sum(tokens) * num_dps (original expressions) */
+  int64_t node_evals_executed;  /* node-evals actually computed (cache skips some) */
+  int32_t kernel_launches;      /* launches of this library's kernels         */
+  int32_t cache_slots_used;
+  int32_t dpt;                  /* launch shape used                          */
+  int32_t warps_per_block;
+  int32_t blocks;
+  int32_t work_items;
+  /* Declared work of one launch of the main kernel (roofline model: operator
+   * counts per datapoint summed over expressions, times num_dps). */
+  double declared_sfu_ops;
+  double declared_fp32_ops;
+  /* Bytes copied host->device / device->host by the call. */
+  int64_t h2d_bytes;
+  int64_t d2h_bytes;
+} sr_stats;
+
+/* ---- lifecycle (reference create_gpu_context / destroy_gpu_context,
+ *      cl_gpu_eval.cu:569-575; create/destroy_gpu_simple_context,
+ *      cl_gpu_simple.cu:315-321) ------------------------------------------- */
+sr_status sr_options_init(sr_options *opts);
+sr_status sr_create(const sr_options *opts, sr_context **out);
+sr_status sr_destroy(sr_context *ctx);
+const char *sr_status_string(sr_status s);
+/* Message of the last failed call on ctx ("" if none). */
+const char *sr_last_error(const sr_context *ctx);
+int32_t sr_abi_version(void);
+
+/* ---- dataset (reference upload_X branch, cl_gpu_eval.cu:474-489) --------
+ * X: host pointer, column-major [(num_vars+1) x num_dps], y in the last row.
+ * The data stays on the device until replaced. */
+sr_status sr_set_data(sr_context *ctx, const float *X, int32_t num_vars,
+                      int64_t num_dps);
+/* Same from the reference's row-pointer form all_vars[0][v][dp] (v <= num_vars). */
+sr_status sr_set_data_rows(sr_context *ctx, const float *const *rows,
+                           int32_t num_vars, int64_t num_dps);
+/* Same from a device pointer (row stride ld >= num_dps floats). */
+sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld,
+                             int32_t num_vars, int64_t num_dps);
+
+/* ---- forward MSE (reference evaluate_gpu_mse, cl_gpu_eval.cu:332-564;
+ *      evaluate_gpu_simple, cl_gpu_simple.cu:187-310) -----------------------
+ * mse_out[i] = sum over valid dps of (pred - y)^2 / count, valid = pred is
+ * neither NaN nor +-Inf; NaN when no datapoint is valid.  num_exprs == 0
+ * returns SR_OK without touching mse_out (reference cl_gpu_eval.cu:342). */
+sr_status sr_eval_mse(sr_context *ctx, const sr_population *pop,
+                      uint32_t flags, float *mse_out, sr_stats *stats);
+
+/* Two-phase form of sr_eval_mse for callers that evaluate the same compiled
+ * population repeatedly: sr_prepare validates, compiles and uploads;
+ * sr_launch enqueues the device work on the context stream (asynchronous);
+ * sr_read_mse waits and copies the result. */
+sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags);
+sr_status sr_launch(sr_context *ctx);
+sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats);
+/* Device times of the most recent sr_launch, after it completed: the whole
+ * launch sequence and the main interpreter kernel alone (CUDA events on the
+ * context stream). */
+sr_status sr_last_launch_times(sr_context *ctx, float *launch_ms, float *eval_kernel_ms);
+/* Device pointer of the MSE vector written by sr_launch (num_exprs floats). */
+sr_status sr_device_mse(sr_context *ctx, float **mse_dev);
+
+/* Per-datapoint predictions of every expression for dps [dp_begin,
+ * dp_begin+dp_count): pred_out[i * dp_count + j].  Predictions are the raw
+ * FP32 stack result, NaN/Inf included (reference evaluate_single_expr,
+ * cl_cpu_eval.cpp:59-90). */
+sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop,
+                              int64_t dp_begin, int64_t dp_count,
+                              float *pred_out);
+
+/* ---- reverse-mode adjoint (no reference counterpart) ----------------------
+ * Constants are the SR_TOK_CONST tokens of each expression, in token order;
+ * grad_out uses the same CSR layout as the constants themselves: for
+ * expression i its constants are numbered from const_offsets[i], where
+ * const_offsets is the exclusive prefix sum of the per-expression constant
+ * counts (sr_count_constants).  grad_out[k] = d mse_i / d c_k. */
+#define SR_GRAD_RECOMPUTE 0 /* forward values recomputed per tile (fused)   */
+#define SR_GRAD_CHECKPOINT 1 /* forward values kept from a separate pass    */
+sr_status sr_count_constants(const sr_population *pop, int64_t *const_offsets);
+sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode,
+                       float *mse_out, float *grad_out, sr_stats *stats);
+
+/* On-device Adam over every expression's constants (steps iterations of
+ * fused forward+adjoint then an Adam update); const_out receives the final
+ * constants (CSR as above), mse_out the MSE at those constants. */
+typedef struct sr_adam_options {
+  int32_t steps;
+  int32_t mode; /* SR_GRAD_RECOMPUTE or SR_GRAD_CHECKPOINT */
+  float lr, beta1, beta2, eps;
+} sr_adam_options;
+sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
+                                const sr_adam_options *adam, float *const_out,
+                                float *mse_out, sr_stats *stats);
+
+/* ---- host-side subtree keys and detection (no device needed) -------------- */
+/* Flat cache key of a token/value run: h = 14695981039346656037; per token
+ * h ^= (uint64)(int64)token; h *= 1099511628211; h ^= bits(double value);
+ * h *= 1099511628211 (reference compute_subtree_hash_gpu,
+ * src/cleaned/cl_gpu_eval.cu:259-272 = compute_hash, src/utils/detect.cpp:50-68). */
+uint64_t sr_subtree_key(const int32_t *tokens, const double *values, int32_t len);
+/* Per-position subtree sizes and Merkle hashes of one expression (reference
+ * detect_common_subtrees reverse pass, src/utils/detect.cpp:169-191, with
+ * hash_node / combine_hashes, detect.cpp:97-118). */
+sr_status sr_subtree_hashes(const int32_t *tokens, const double *values, int32_t len,
+                            int32_t *sizes, uint64_t *hashes);
+
+typedef struct sr_detect_result {
+  int32_t num_subtrees;     /* groups found                                 */
+  int32_t reserved0;
+  int64_t total_tokens;
+  int64_t covered_tokens;   /* tokens under the greedy non-overlapping cover */
+  double avg_subtree_size;
+  double coverage;          /* covered_tokens / total_tokens                */
+} sr_detect_result;
+
+/* Common-subtree detection (reference detect_common_subtrees,
+ * src/utils/detect.cpp:120-387).  Groups come out largest first; for group g
+ * (g < max_groups) the optional arrays receive its representative occurrence
+ * (expression, position), size, verified occurrence count and flat key. */
+sr_status sr_detect_subtrees(const sr_population *pop, int32_t min_size, int32_t min_freq,
+                             int32_t max_groups, sr_detect_result *res, int32_t *group_expr,
+                             int32_t *group_pos, int32_t *group_size, int32_t *group_count,
+                             uint64_t *group_key);
+
+/* Cache marking (reference mark_cached_subtrees_from_state,
+ * src/cleaned/cl_gpu_eval.cu:294-329): given cached keys and their slots,
+ * hints[t] for every token t of pop is the slot at the root of a cached
+ * subtree, -2 on its body, -1 elsewhere (outermost subtree of >= 3 tokens wins). */
+sr_status sr_mark_cached(const sr_population *pop, const uint64_t *keys, const int32_t *slots,
+                         int32_t n_keys, int32_t *hints);
+
+/* Validate a population and report per-expression bytecode size and spill
+ * slots (either output may be NULL).  First error wins; sr_last_error is not
+ * available here, so the failing expression index goes to *bad_expr. */
+sr_status sr_validate_population(const sr_population *pop, int32_t num_vars,
+                                 int32_t *n_instr, int32_t *spill_slots, int32_t *bad_expr);
+
+/* ---- misc ------------------------------------------------------------------ */
+sr_status sr_get_stream(sr_context *ctx, void **stream);
+sr_status sr_synchronize(sr_context *ctx);
+/* Measured per-SM pipe peaks on this device (FP32 FMA lanes/clock and MUFU
+ * ex2 lanes/clock) from two short microbenchmarks, plus the SM count. */
+sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s,
+                           double *sfu_ops_per_s, int32_t *num_sms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SR_EVAL_H */

@@ -1,0 +1,1093 @@
+// sr_capi.cpp — the C ABI (sr_eval.h): context lifecycle, dataset upload,
+// population compilation / planning / upload, launches and read-back.
+//
+// Reference counterpart: evaluate_gpu_mse (src/cleaned/cl_gpu_eval.cu:332-564)
+// and evaluate_gpu_simple (src/cleaned/cl_gpu_simple.cu:187-310).  Where the
+// reference synchronises after every copy and kernel and exits the process
+// on a CUDA error, this runtime compiles on host threads, issues pinned
+// asynchronous copies and all kernels back to back on one stream, waits once,
+// and reports failures as status codes.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <sstream>
+#include <thread>
+
+#include "sr_context.hpp"
+#include "sr_kernels.hpp"
+
+using sr::Instr;
+using sr::ProgramSet;
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+sr_status cuda_fail(sr_context *ctx, cudaError_t e, const char *what) {
+  const sr_status s = (e == cudaErrorMemoryAllocation) ? SR_ERR_OUT_OF_MEMORY : SR_ERR_CUDA;
+  return ctx->fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SR_TRY_CUDA(ctx, call)                              \
+  do {                                                      \
+    const cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+#define SR_TRY(call)                  \
+  do {                                \
+    const sr_status s_ = (call);      \
+    if (s_ != SR_OK) return s_;       \
+  } while (0)
+
+// Makes ctx->device current for the scope of an API call.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int host_threads(const sr_context *ctx) {
+  int t = ctx->opts.host_threads;
+  if (t <= 0) t = static_cast<int>(std::thread::hardware_concurrency());
+  return std::max(1, std::min(t, 64));
+}
+
+int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+sr_status check_population(sr_context *ctx, const sr_population *pop) {
+  if (!pop) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "population is NULL");
+  if (pop->num_exprs < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "num_exprs < 0");
+  if (pop->num_exprs == 0) return SR_OK;
+  if (!pop->tokens || !pop->values || !pop->offsets)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "population arrays must not be NULL");
+  if (pop->offsets[0] != 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+  for (int i = 0; i < pop->num_exprs; ++i) {
+    const int64_t len = pop->offsets[i + 1] - pop->offsets[i];
+    if (len <= 0)
+      return ctx->fail(SR_ERR_MALFORMED_EXPRESSION,
+                       "expression " + std::to_string(i) + " is empty");
+    if (len > SR_MAX_TOKENS)
+      return ctx->fail(SR_ERR_EXPRESSION_TOO_LONG,
+                       "expression " + std::to_string(i) + " has " + std::to_string(len) +
+                           " tokens (max " + std::to_string(SR_MAX_TOKENS) + ")");
+  }
+  return SR_OK;
+}
+
+// Compile expressions [0, E) of a CSR population into ps (pinned staging).
+sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *val,
+                      const int64_t *off, const int32_t *hints, ProgramSet &ps) {
+  ps.E = E;
+  ps.cost.assign(static_cast<size_t>(E), 0.f);
+  ps.smax = 0;
+  ps.n_instr = 0;
+  ps.n_tokens = 0;
+  ps.sfu_per_dp = ps.fp32_per_dp = 0.0;
+  const int nt = std::max(1, std::min(host_threads(ctx), std::max(1, E / 32)));
+  std::vector<std::vector<Instr>> codes(static_cast<size_t>(nt));
+  std::vector<sr::ExprInfo> infos(static_cast<size_t>(E));
+  std::vector<sr_status> st(static_cast<size_t>(nt), SR_OK);
+  std::vector<std::string> msg(static_cast<size_t>(nt));
+  std::vector<int64_t> bad(static_cast<size_t>(nt), -1);
+  sr::parallel_for(nt, nt, [&](int64_t b, int64_t e) {
+    for (int64_t c = b; c < e; ++c) {
+      const int64_t x0 = static_cast<int64_t>(E) * c / nt, x1 = static_cast<int64_t>(E) * (c + 1) / nt;
+      auto &code = codes[static_cast<size_t>(c)];
+      code.reserve(static_cast<size_t>((off[x1] - off[x0]) / 2 + 8));
+      for (int64_t x = x0; x < x1; ++x) {
+        std::string err;
+        const sr_status s = sr::compile_expression(
+            tok + off[x], val + off[x], static_cast<int>(off[x + 1] - off[x]), ctx->V,
+            hints ? hints + off[x] : nullptr, code, infos[static_cast<size_t>(x)], &err);
+        if (s != SR_OK) {
+          st[static_cast<size_t>(c)] = s;
+          msg[static_cast<size_t>(c)] = err;
+          bad[static_cast<size_t>(c)] = x;
+          return;
+        }
+      }
+    }
+  });
+  for (int c = 0; c < nt; ++c)
+    if (st[static_cast<size_t>(c)] != SR_OK)
+      return ctx->fail(st[static_cast<size_t>(c)],
+                       "expression " + std::to_string(bad[static_cast<size_t>(c)]) + ": " +
+                           msg[static_cast<size_t>(c)]);
+  int64_t total = 0;
+  for (auto &c : codes) total += static_cast<int64_t>(c.size());
+  SR_TRY_CUDA(ctx, ps.h_code.ensure(static_cast<size_t>(total + 1)));
+  SR_TRY_CUDA(ctx, ps.h_off.ensure(static_cast<size_t>(std::max(E, 1))));
+  SR_TRY_CUDA(ctx, ps.h_len.ensure(static_cast<size_t>(std::max(E, 1))));
+  int64_t pos = 0;
+  for (auto &c : codes) {
+    std::memcpy(ps.h_code.p + pos, c.data(), c.size() * sizeof(Instr));
+    pos += static_cast<int64_t>(c.size());
+  }
+  ps.h_code.p[total] = Instr{0, 0, 0, 0};  // prefetch padding
+  int64_t o = 0;
+  for (int x = 0; x < E; ++x) {
+    const auto &in = infos[static_cast<size_t>(x)];
+    ps.h_off.p[x] = o;
+    ps.h_len.p[x] = in.n_instr;
+    o += in.n_instr;
+    ps.cost[static_cast<size_t>(x)] = in.cost;
+    ps.smax = std::max(ps.smax, in.need);
+    ps.n_tokens += in.n_tokens;
+    ps.sfu_per_dp += in.sfu_ops;
+    ps.fp32_per_dp += in.fp32_ops;
+  }
+  ps.n_instr = total;
+  return SR_OK;
+}
+
+// Launch shape: groups of W cost-sorted expressions x spans of tiles.
+sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W) {
+  sr::Plan p;
+  p.dpt = dpt;
+  p.W = W;
+  p.smax = std::max(ps.smax, 0);
+  const int64_t tile = 32 * dpt;
+  const int E = ps.E;
+  p.n_tiles = static_cast<int>((ctx->N + tile - 1) / tile);
+  p.n_groups = (E + W - 1) / W;
+  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.smax);
+  int dev_max_smem = 0;
+  cudaDeviceGetAttribute(&dev_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+  if (p.smem > static_cast<size_t>(dev_max_smem))
+    return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape needs " + std::to_string(p.smem) +
+                                             " bytes of shared memory");
+  int bps = 0;
+  SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.smem, W, &bps));
+  if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
+  const int64_t resident = static_cast<int64_t>(bps) * ctx->num_sms;
+  if (p.n_tiles == 0 || E == 0) {
+    p.n_spans = 0;
+    p.tiles_per_span = 0;
+  } else {
+    const int64_t target = 8 * resident;
+    int64_t spans = (target + p.n_groups - 1) / p.n_groups;
+    spans = std::max<int64_t>(1, std::min<int64_t>(spans, p.n_tiles));
+    if (!pred) {
+      const int64_t cap = std::max<int64_t>(1, (int64_t{1} << 28) / (16 * static_cast<int64_t>(E)));
+      spans = std::min(spans, cap);
+    }
+    // Per-warp datapoint counts stay below 2^30 (int counters).
+    const int64_t min_spans = (static_cast<int64_t>(p.n_tiles) * tile + (int64_t{1} << 30) - 1) >> 30;
+    spans = std::max(spans, min_spans);
+    const int64_t tps = (p.n_tiles + spans - 1) / spans;
+    p.tiles_per_span = static_cast<int>(tps);
+    p.n_spans = static_cast<int>((p.n_tiles + tps - 1) / tps);
+  }
+  p.blocks = static_cast<int>(std::min<int64_t>(resident, std::max<int64_t>(p.items(), 1)));
+  // Group table: expressions in decreasing modelled cost, W per group.
+  SR_TRY_CUDA(ctx, ps.h_group.ensure(static_cast<size_t>(std::max(p.n_groups * W, 1))));
+  std::vector<int32_t> order(static_cast<size_t>(E));
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+    return ps.cost[static_cast<size_t>(a)] > ps.cost[static_cast<size_t>(b)];
+  });
+  for (int64_t k = 0; k < static_cast<int64_t>(p.n_groups) * W; ++k)
+    ps.h_group.p[k] = k < E ? order[static_cast<size_t>(k)] : -1;
+  ps.plan = p;
+  return SR_OK;
+}
+
+sr_status upload_groups(sr_context *ctx, ProgramSet &ps) {
+  const size_t ng = static_cast<size_t>(std::max(ps.plan.n_groups * ps.plan.W, 1));
+  ctx->prep_stats.h2d_bytes += static_cast<int64_t>(ng * sizeof(int32_t));
+  SR_TRY_CUDA(ctx, ps.group.ensure(ng));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.group.p, ps.h_group.p, ng * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  return SR_OK;
+}
+
+sr_status upload_code(sr_context *ctx, ProgramSet &ps) {
+  const int E = ps.E;
+  SR_TRY_CUDA(ctx, ps.code.ensure(static_cast<size_t>(ps.n_instr + 1)));
+  SR_TRY_CUDA(ctx, ps.off.ensure(static_cast<size_t>(std::max(E, 1))));
+  SR_TRY_CUDA(ctx, ps.len.ensure(static_cast<size_t>(std::max(E, 1))));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.code.p, ps.h_code.p, (ps.n_instr + 1) * sizeof(Instr),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  ctx->prep_stats.h2d_bytes += static_cast<int64_t>((ps.n_instr + 1) * sizeof(Instr)) +
+                               static_cast<int64_t>(E) * (sizeof(int64_t) + sizeof(int32_t));
+  if (E > 0) {
+    SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.off.p, ps.h_off.p, E * sizeof(int64_t),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.len.p, ps.h_len.p, E * sizeof(int32_t),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+  }
+  return SR_OK;
+}
+
+sr::EvalArgs make_args(sr_context *ctx, ProgramSet &ps, int32_t *counter) {
+  sr::EvalArgs a{};
+  a.X = ctx->X.p;
+  a.ldx = ctx->ldx;
+  a.N = ctx->N;
+  a.code = ps.code.p;
+  a.code_off = ps.off.p;
+  a.code_len = ps.len.p;
+  a.group_expr = ps.group.p;
+  a.partial = ctx->partial.p;
+  a.work_counter = counter;
+  a.error = ctx->d_error;
+  a.cache = ctx->cache_vals.p;
+  a.ldc = ctx->ldx;
+  a.V = ctx->V;
+  a.E = ps.E;
+  a.W = ps.plan.W;
+  a.smax = ps.plan.smax;
+  a.n_groups = ps.plan.n_groups;
+  a.n_spans = ps.plan.n_spans;
+  a.tiles_per_span = ps.plan.tiles_per_span;
+  a.n_tiles = ps.plan.n_tiles;
+  return a;
+}
+
+sr_status launch_set(sr_context *ctx, ProgramSet &ps, bool pred, int32_t *counter,
+                     float *pred_out, int64_t ldp, const int32_t *pred_row) {
+  if (ps.plan.items() == 0) return SR_OK;
+  sr::EvalArgs a = make_args(ctx, ps, counter);
+  a.pred = pred_out;
+  a.ldp = ldp;
+  a.pred_row = pred_row;
+  SR_TRY_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int32_t), ctx->stream));
+  SR_TRY_CUDA(ctx, sr::launch_interp(ps.plan.dpt, pred, a, ps.plan.blocks, ps.plan.smem,
+                                     ctx->stream));
+  return SR_OK;
+}
+
+// ---- launch-shape tuning ---------------------------------------------------
+
+std::string tune_key(const sr_context *ctx, const ProgramSet &ps) {
+  const int lg_n = ctx->N > 0 ? static_cast<int>(std::log2(static_cast<double>(ctx->N))) : 0;
+  const int lg_e = ps.E > 0 ? static_cast<int>(std::log2(static_cast<double>(ps.E))) : 0;
+  const double mean_instr = ps.E > 0 ? static_cast<double>(ps.n_instr) / ps.E : 0.0;
+  std::ostringstream k;
+  k << ctx->device_name << "|V" << ctx->V << "|N" << lg_n << "|E" << lg_e << "|I"
+    << static_cast<int>(std::lround(std::log2(1.0 + mean_instr) * 4.0)) << "|S" << ps.smax;
+  return k.str();
+}
+
+void load_tune_cache(sr_context *ctx) {
+  ctx->tune_loaded = true;
+  if (!ctx->opts.tune_cache_path) return;
+  std::ifstream f(ctx->opts.tune_cache_path);
+  if (!f) return;
+  // Format: one entry per line:  "key": [dpt, W],
+  std::string line;
+  while (std::getline(f, line)) {
+    const size_t q0 = line.find('"'), q1 = line.find('"', q0 + 1);
+    const size_t b0 = line.find('[', q1), b1 = line.find(']', b0);
+    if (q0 == std::string::npos || q1 == std::string::npos || b0 == std::string::npos ||
+        b1 == std::string::npos)
+      continue;
+    int dpt = 0, w = 0;
+    if (std::sscanf(line.c_str() + b0, "[%d, %d]", &dpt, &w) == 2 && (dpt == 4 || dpt == 8) &&
+        w >= 1 && w <= sr::kMaxWarps)
+      ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w};
+  }
+}
+
+void save_tune_cache(const sr_context *ctx) {
+  if (!ctx->opts.tune_cache_path) return;
+  std::ofstream f(ctx->opts.tune_cache_path, std::ios::trunc);
+  if (!f) return;
+  f << "{\n";
+  size_t i = 0;
+  for (const auto &kv : ctx->tuned) {
+    f << "  \"" << kv.first << "\": [" << kv.second.first << ", " << kv.second.second << "]"
+      << (++i < ctx->tuned.size() ? "," : "") << "\n";
+  }
+  f << "}\n";
+}
+
+// Times each candidate shape on the prepared population and keeps the fastest.
+sr_status autotune_main(sr_context *ctx, const std::string &key) {
+  static const int kCand[][2] = {{8, 8}, {8, 6}, {8, 4}, {4, 8}, {4, 4}};
+  float best = 1e30f;
+  int best_dpt = 8, best_w = 8;
+  cudaEvent_t a = ctx->ev[4], b = ctx->ev[5];
+  for (const auto &c : kCand) {
+    if (plan_set(ctx, ctx->main, false, c[0], c[1]) != SR_OK) continue;
+    SR_TRY(upload_groups(ctx, ctx->main));
+    SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(std::max<int64_t>(
+                         static_cast<int64_t>(ctx->main.plan.n_spans) * ctx->main.E, 1))));
+    float t_sum = 0.f;
+    for (int rep = 0; rep < 3; ++rep) {
+      SR_TRY_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+      SR_TRY(launch_set(ctx, ctx->main, false, ctx->d_counter, nullptr, 0, nullptr));
+      SR_TRY_CUDA(ctx, cudaEventRecord(b, ctx->stream));
+      SR_TRY_CUDA(ctx, cudaEventSynchronize(b));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0) t_sum += ms;  // first run warms up
+    }
+    if (t_sum < best) {
+      best = t_sum;
+      best_dpt = c[0];
+      best_w = c[1];
+    }
+  }
+  ctx->tuned[key] = {best_dpt, best_w};
+  save_tune_cache(ctx);
+  return SR_OK;
+}
+
+sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
+  ProgramSet &ps = ctx->main;
+  int dpt = ctx->opts.dpt, W = ctx->opts.warps_per_block;
+  if (dpt == 0 || W == 0) {
+    if (!ctx->tune_loaded) load_tune_cache(ctx);
+    const std::string key = tune_key(ctx, ps);
+    auto it = ctx->tuned.find(key);
+    if (it == ctx->tuned.end() && allow_tune && ctx->opts.autotune && ps.E > 0 && ctx->N > 0) {
+      SR_TRY(autotune_main(ctx, key));
+      it = ctx->tuned.find(key);
+    }
+    const int tdpt = it != ctx->tuned.end() ? it->second.first : 8;
+    const int tw = it != ctx->tuned.end() ? it->second.second : 8;
+    if (dpt == 0) dpt = tdpt;
+    if (W == 0) W = tw;
+  }
+  SR_TRY(plan_set(ctx, ps, false, dpt, W));
+  SR_TRY(upload_groups(ctx, ps));
+  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
+                       std::max<int64_t>(static_cast<int64_t>(ps.plan.n_spans) * ps.E, 1))));
+  return SR_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+int32_t sr_abi_version(void) { return SR_ABI_VERSION; }
+
+const char *sr_status_string(sr_status s) {
+  switch (s) {
+    case SR_OK: return "ok";
+    case SR_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case SR_ERR_BAD_TOKEN: return "unknown token";
+    case SR_ERR_MALFORMED_EXPRESSION: return "malformed expression";
+    case SR_ERR_EXPRESSION_TOO_LONG: return "expression too long";
+    case SR_ERR_NO_DATA: return "no dataset on the device";
+    case SR_ERR_CUDA: return "CUDA error";
+    case SR_ERR_OUT_OF_MEMORY: return "out of memory";
+    case SR_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+    case SR_ERR_DEVICE_CHECK: return "device bounds check failed";
+    case SR_ERR_UNSUPPORTED: return "unsupported";
+    case SR_ERR_NO_DEVICE: return "no CUDA device";
+    case SR_ERR_TOO_MANY_VARS: return "too many variables";
+  }
+  return "unknown status";
+}
+
+const char *sr_last_error(const sr_context *ctx) {
+  return ctx ? ctx->last_error.c_str() : "";
+}
+
+sr_status sr_options_init(sr_options *o) {
+  if (!o) return SR_ERR_INVALID_ARGUMENT;
+  std::memset(o, 0, sizeof *o);
+  o->device = -1;
+  o->cache_capacity = 2048;
+  o->min_subtree_size = 3;
+  o->min_subtree_freq = 10;
+  o->dpt = 0;
+  o->warps_per_block = 0;
+  o->autotune = 0;
+  o->use_graphs = 0;
+  o->host_threads = 0;
+  o->tune_cache_path = nullptr;
+  o->stream = nullptr;
+  return SR_OK;
+}
+
+sr_status sr_create(const sr_options *opts, sr_context **out) {
+  if (!out) return SR_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  sr_options o;
+  if (opts) o = *opts;
+  else sr_options_init(&o);
+  if (o.dpt != 0 && o.dpt != 4 && o.dpt != 8) return SR_ERR_INVALID_ARGUMENT;
+  if (o.warps_per_block < 0 || o.warps_per_block > sr::kMaxWarps) return SR_ERR_INVALID_ARGUMENT;
+  if (o.cache_capacity < 0 || o.min_subtree_size < 1 || o.min_subtree_freq < 1)
+    return SR_ERR_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    return SR_ERR_NO_DEVICE;
+  }
+  int dev = o.device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return SR_ERR_NO_DEVICE;
+  if (dev >= ndev) return SR_ERR_INVALID_ARGUMENT;
+  auto *ctx = new sr_context();
+  ctx->opts = o;
+  ctx->device = dev;
+  DeviceScope scope(dev);
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major < 10) {
+    delete ctx;
+    return SR_ERR_NO_DEVICE;  // this build carries sm_100a code only
+  }
+  ctx->num_sms = prop.multiProcessorCount;
+  ctx->device_name = prop.name;
+  ctx->cache.capacity = o.cache_capacity;
+  cudaError_t e = cudaSuccess;
+  if (o.stream) {
+    ctx->stream = static_cast<cudaStream_t>(o.stream);
+  } else {
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    ctx->own_stream = (e == cudaSuccess);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counter, 2 * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_error, 0, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_error, sizeof(int32_t));
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+  if (e != cudaSuccess) {
+    sr_destroy(ctx);
+    return e == cudaErrorMemoryAllocation ? SR_ERR_OUT_OF_MEMORY : SR_ERR_CUDA;
+  }
+  *out = ctx;
+  return SR_OK;
+}
+
+sr_status sr_destroy(sr_context *ctx) {
+  if (!ctx) return SR_OK;
+  DeviceScope scope(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &ev : ctx->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (ctx->d_counter) cudaFree(ctx->d_counter);
+  if (ctx->d_error) cudaFree(ctx->d_error);
+  if (ctx->h_error) cudaFreeHost(ctx->h_error);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;  // device and pinned buffers are released by their owners
+  return SR_OK;
+}
+
+sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, int32_t num_vars,
+                             int64_t num_dps) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (num_vars < 0 || num_dps < 0 || (num_dps > 0 && !X_dev) || ld < num_dps)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad dataset arguments");
+  if (num_vars > SR_MAX_VARS)
+    return ctx->fail(SR_ERR_TOO_MANY_VARS, "num_vars " + std::to_string(num_vars) +
+                                               " exceeds " + std::to_string(SR_MAX_VARS));
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int64_t ldx = std::max<int64_t>(1024, round_up(num_dps, 1024));
+  const size_t rows = static_cast<size_t>(num_vars) + 1;
+  SR_TRY_CUDA(ctx, ctx->X.ensure(rows * static_cast<size_t>(ldx)));
+  SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->X.p, 0, rows * ldx * sizeof(float), ctx->stream));
+  if (num_dps > 0)
+    SR_TRY_CUDA(ctx, cudaMemcpy2DAsync(ctx->X.p, ldx * sizeof(float), X_dev, ld * sizeof(float),
+                                       num_dps * sizeof(float), rows, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->ldx = ldx;
+  ctx->V = num_vars;
+  ctx->N = num_dps;
+  ctx->cache.clear();  // cached subtree values belong to the old data
+  ctx->mode = sr::Mode::kNone;
+  return SR_OK;
+}
+
+static sr_status set_data_host(sr_context *ctx, const float *X, const float *const *rows_ptr,
+                               int32_t num_vars, int64_t num_dps) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (num_vars < 0 || num_dps < 0 || (num_dps > 0 && !X && !rows_ptr))
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad dataset arguments");
+  if (num_vars > SR_MAX_VARS)
+    return ctx->fail(SR_ERR_TOO_MANY_VARS, "num_vars " + std::to_string(num_vars) +
+                                               " exceeds " + std::to_string(SR_MAX_VARS));
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int64_t ldx = std::max<int64_t>(1024, round_up(num_dps, 1024));
+  const size_t rows = static_cast<size_t>(num_vars) + 1;
+  SR_TRY_CUDA(ctx, ctx->X.ensure(rows * static_cast<size_t>(ldx)));
+  SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->X.p, 0, rows * ldx * sizeof(float), ctx->stream));
+  if (num_dps > 0) {
+    if (X) {
+      SR_TRY_CUDA(ctx, cudaMemcpy2DAsync(ctx->X.p, ldx * sizeof(float), X,
+                                         num_dps * sizeof(float), num_dps * sizeof(float), rows,
+                                         cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+      for (size_t v = 0; v < rows; ++v) {
+        if (!rows_ptr[v]) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "data row is NULL");
+        SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->X.p + v * ldx, rows_ptr[v], num_dps * sizeof(float),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+      }
+    }
+  }
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->ldx = ldx;
+  ctx->V = num_vars;
+  ctx->N = num_dps;
+  ctx->cache.clear();
+  ctx->mode = sr::Mode::kNone;
+  return SR_OK;
+}
+
+sr_status sr_set_data(sr_context *ctx, const float *X, int32_t num_vars, int64_t num_dps) {
+  return set_data_host(ctx, X, nullptr, num_vars, num_dps);
+}
+
+sr_status sr_set_data_rows(sr_context *ctx, const float *const *rows, int32_t num_vars,
+                           int64_t num_dps) {
+  if (ctx && num_dps > 0 && !rows) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "rows is NULL");
+  return set_data_host(ctx, nullptr, rows, num_vars, num_dps);
+}
+
+// ---- prepare --------------------------------------------------------------
+
+static sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
+  sr::PlainSet &ps = ctx->plain;
+  const int E = pop->num_exprs;
+  const int64_t T = pop->offsets[E];
+  // Validate through the compiler (same rules as the batched path) and check
+  // the raw stack depth against the plain kernel's local stack.
+  std::vector<Instr> scratch;
+  for (int x = 0; x < E; ++x) {
+    const int64_t o = pop->offsets[x];
+    const int len = static_cast<int>(pop->offsets[x + 1] - o);
+    sr::ExprInfo info;
+    std::string err;
+    scratch.clear();
+    const sr_status s = sr::compile_expression(pop->tokens + o, pop->values + o, len, ctx->V,
+                                               nullptr, scratch, info, &err);
+    if (s != SR_OK) return ctx->fail(s, "expression " + std::to_string(x) + ": " + err);
+    int depth = 0, maxd = 0;
+    for (int i = len - 1; i >= 0; --i) {
+      const int t = pop->tokens[o + i];
+      if (t <= 0) ++depth;
+      else if (sr::is_binary_token(t)) --depth;
+      maxd = std::max(maxd, depth);
+    }
+    if (maxd > sr::kPlainStack)
+      return ctx->fail(SR_ERR_UNSUPPORTED, "expression " + std::to_string(x) +
+                                               " exceeds the plain kernel's stack");
+  }
+  SR_TRY_CUDA(ctx, ps.h_tok.ensure(static_cast<size_t>(T)));
+  SR_TRY_CUDA(ctx, ps.h_val.ensure(static_cast<size_t>(T)));
+  SR_TRY_CUDA(ctx, ps.h_off.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ps.h_len.ensure(static_cast<size_t>(E)));
+  for (int64_t i = 0; i < T; ++i) {
+    const int t = pop->tokens[i];
+    const double v = pop->values[i];
+    ps.h_tok.p[i] = t;
+    if (t == SR_TOK_VAR) {
+      const bool ok = v > -2147483648.0 && v < 2147483648.0;
+      const int vi = ok ? static_cast<int>(v) : -1;
+      ps.h_val.p[i] = static_cast<float>((vi >= 0 && vi < ctx->V) ? vi : -1);
+    } else {
+      ps.h_val.p[i] = static_cast<float>(v);
+    }
+  }
+  for (int x = 0; x < E; ++x) {
+    ps.h_off.p[x] = pop->offsets[x];
+    ps.h_len.p[x] = static_cast<int32_t>(pop->offsets[x + 1] - pop->offsets[x]);
+  }
+  SR_TRY_CUDA(ctx, ps.tok.ensure(static_cast<size_t>(T)));
+  SR_TRY_CUDA(ctx, ps.val.ensure(static_cast<size_t>(T)));
+  SR_TRY_CUDA(ctx, ps.off.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ps.len.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.tok.p, ps.h_tok.p, T * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.val.p, ps.h_val.p, T * sizeof(float),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.off.p, ps.h_off.p, E * sizeof(int64_t),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.len.p, ps.h_len.p, E * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  ps.E = E;
+  ctx->prep_stats.h2d_bytes += T * static_cast<int64_t>(sizeof(int32_t) + sizeof(float)) +
+                               static_cast<int64_t>(E) * (sizeof(int64_t) + sizeof(int32_t));
+  ps.n_dpblocks = static_cast<int>(std::min<int64_t>((ctx->N + 127) / 128, 256));
+  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
+                       std::max<int64_t>(static_cast<int64_t>(ps.n_dpblocks) * E, 1))));
+  ctx->prep_stats.node_evals = T * ctx->N;
+  ctx->prep_stats.node_evals_executed = T * ctx->N;
+  return SR_OK;
+}
+
+static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint32_t flags) {
+  const int E = pop->num_exprs;
+  const int64_t T = pop->offsets[E];
+  // Validate first so that malformed input never reaches the cache.
+  {
+    std::vector<Instr> scratch;
+    for (int x = 0; x < E; ++x) {
+      const int64_t o = pop->offsets[x];
+      sr::ExprInfo info;
+      std::string err;
+      scratch.clear();
+      const sr_status s = sr::compile_expression(pop->tokens + o, pop->values + o,
+                                                 static_cast<int>(pop->offsets[x + 1] - o), ctx->V,
+                                                 nullptr, scratch, info, &err);
+      if (s != SR_OK) return ctx->fail(s, "expression " + std::to_string(x) + ": " + err);
+    }
+  }
+  if (flags & SR_EVAL_CLEAR_CACHE) ctx->cache.clear();
+  const int threads = host_threads(ctx);
+  const double t0 = now_ms();
+  sr::Detection det;
+  sr::detect_common_subtrees(E, pop->tokens, pop->values, pop->offsets,
+                             ctx->opts.min_subtree_size, ctx->opts.min_subtree_freq, threads, det);
+  ctx->prep_stats.detect_time_ms = now_ms() - t0;
+  ctx->prep_stats.num_subtrees = static_cast<int32_t>(det.groups.size());
+  ctx->prep_stats.avg_subtree_size = det.avg_subtree_size;
+  ctx->prep_stats.coverage = det.coverage;
+
+  // Cache update (reference cl_gpu_eval.cu:384-396): new keys get the next
+  // free slot until the capacity is reached.
+  std::vector<int32_t> sub_tok;
+  std::vector<double> sub_val;
+  std::vector<int64_t> sub_off{0};
+  std::vector<int32_t> sub_slot;
+  for (const auto &g : det.groups) {
+    const int32_t *t = pop->tokens + pop->offsets[g.expr] + g.pos;
+    const double *v = pop->values + pop->offsets[g.expr] + g.pos;
+    const uint64_t key = sr::flat_key(t, v, g.size);
+    if (ctx->cache.slot_of.count(key)) continue;
+    if (ctx->cache.used >= ctx->cache.capacity) continue;
+    const int32_t slot = ctx->cache.used++;
+    ctx->cache.slot_of.emplace(key, slot);
+    sub_tok.insert(sub_tok.end(), t, t + g.size);
+    sub_val.insert(sub_val.end(), v, v + g.size);
+    sub_off.push_back(static_cast<int64_t>(sub_tok.size()));
+    sub_slot.push_back(slot);
+  }
+  const int n_new = static_cast<int>(sub_slot.size());
+  ctx->prep_stats.new_subtrees = n_new;
+  ctx->prep_stats.cache_slots_used = ctx->cache.used;
+
+  // Cache values live in [capacity][ldx]; allocated on first use.
+  if (ctx->cache.capacity > 0)
+    SR_TRY_CUDA(ctx, ctx->cache_vals.ensure(static_cast<size_t>(ctx->cache.capacity) * ctx->ldx));
+
+  // Subtrees to evaluate into the cache this call.
+  const double tc0 = now_ms();
+  SR_TRY(compile_set(ctx, n_new, sub_tok.data(), sub_val.data(), sub_off.data(), nullptr, ctx->sub));
+  SR_TRY_CUDA(ctx, ctx->sub.h_row.ensure(static_cast<size_t>(std::max(n_new, 1))));
+  for (int k = 0; k < n_new; ++k) ctx->sub.h_row.p[k] = sub_slot[static_cast<size_t>(k)];
+  if (n_new > 0) {
+    SR_TRY(plan_set(ctx, ctx->sub, true, 8, sr::kMaxWarps));
+    SR_TRY(upload_code(ctx, ctx->sub));
+    SR_TRY(upload_groups(ctx, ctx->sub));
+    SR_TRY_CUDA(ctx, ctx->sub.row.ensure(static_cast<size_t>(n_new)));
+    SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->sub.row.p, ctx->sub.h_row.p, n_new * sizeof(int32_t),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    ctx->prep_stats.h2d_bytes += static_cast<int64_t>(n_new) * sizeof(int32_t);
+  } else {
+    ctx->sub.plan = sr::Plan{};
+  }
+
+  // Skeletons (reference mark_cached_subtrees_from_state + skeleton rewrite,
+  // cl_gpu_eval.cu:294-329, 433-459).
+  ctx->hints.resize(static_cast<size_t>(T));
+  const int64_t removed = sr::mark_cached_subtrees(E, pop->tokens, pop->values, pop->offsets,
+                                                   ctx->cache, threads, ctx->hints.data());
+  SR_TRY(compile_set(ctx, E, pop->tokens, pop->values, pop->offsets, ctx->hints.data(), ctx->main));
+  ctx->prep_stats.host_compile_time_ms = now_ms() - tc0;
+  SR_TRY(upload_code(ctx, ctx->main));
+  SR_TRY(prepare_main_shape(ctx, false));
+  ctx->prep_stats.node_evals = T * ctx->N;
+  ctx->prep_stats.node_evals_executed = (T - removed + static_cast<int64_t>(sub_tok.size())) * ctx->N;
+  return SR_OK;
+}
+
+sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  SR_TRY(check_population(ctx, pop));
+  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->mode = sr::Mode::kNone;
+  ctx->prep_stats = sr_stats{};
+  const int E = pop->num_exprs;
+  ctx->E = E;
+  if (E == 0) return SR_OK;
+  SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
+  if (flags & SR_EVAL_PLAIN) {
+    SR_TRY(prepare_plain(ctx, pop));
+    ctx->mode = sr::Mode::kPlain;
+  } else if (flags & SR_EVAL_SUBTREE_CACHE) {
+    SR_TRY(prepare_cached(ctx, pop, flags));
+    ctx->mode = sr::Mode::kCached;
+  } else {
+    const double tc0 = now_ms();
+    SR_TRY(compile_set(ctx, E, pop->tokens, pop->values, pop->offsets, nullptr, ctx->main));
+    ctx->prep_stats.host_compile_time_ms = now_ms() - tc0;
+    SR_TRY(upload_code(ctx, ctx->main));
+    SR_TRY(prepare_main_shape(ctx, true));
+    ctx->prep_stats.node_evals = ctx->main.n_tokens * ctx->N;
+    ctx->prep_stats.node_evals_executed = ctx->prep_stats.node_evals;
+    ctx->mode = sr::Mode::kBatched;
+  }
+  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
+  return SR_OK;
+}
+
+sr_status sr_launch(sr_context *ctx) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (ctx->E == 0) return SR_OK;
+  if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing prepared");
+  DeviceScope scope(ctx->device);
+  cudaStream_t s = ctx->stream;
+  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+  int launches = 0;
+  if (ctx->mode == sr::Mode::kPlain) {
+    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    SR_TRY_CUDA(ctx, sr::launch_plain(ctx->plain.tok.p, ctx->plain.val.p, ctx->plain.off.p,
+                                      ctx->plain.len.p, ctx->X.p, ctx->ldx, ctx->V, ctx->N,
+                                      ctx->plain.E, ctx->partial.p, ctx->plain.n_dpblocks, s));
+    launches += ctx->N > 0 ? 1 : 0;
+    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+    SR_TRY_CUDA(ctx, sr::launch_finalize(ctx->partial.p, ctx->N > 0 ? ctx->plain.n_dpblocks : 0,
+                                         ctx->E, ctx->mse.p, s));
+    ++launches;
+  } else {
+    if (ctx->mode == sr::Mode::kCached && ctx->sub.plan.items() > 0) {
+      SR_TRY(launch_set(ctx, ctx->sub, true, ctx->d_counter + 1, ctx->cache_vals.p, ctx->ldx,
+                        ctx->sub.row.p));
+      ++launches;
+    }
+    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    if (ctx->main.plan.items() > 0) {
+      SR_TRY(launch_set(ctx, ctx->main, false, ctx->d_counter, nullptr, 0, nullptr));
+      ++launches;
+    }
+    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+    SR_TRY_CUDA(ctx, sr::launch_finalize(ctx->partial.p, ctx->main.plan.n_spans, ctx->E,
+                                         ctx->mse.p, s));
+    ++launches;
+  }
+  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[3], s));
+  ctx->timing_valid = true;
+  ctx->prep_stats.kernel_launches = launches;
+  return SR_OK;
+}
+
+static sr_status check_device_error(sr_context *ctx) {
+  if (*ctx->h_error == 0) return SR_OK;
+  const int32_t code = *ctx->h_error;
+  *ctx->h_error = 0;
+  cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  if (code & sr::kDevErrTimeout)
+    return ctx->fail(SR_ERR_DEVICE_TIMEOUT, "a device-side wait exceeded its time limit");
+  return ctx->fail(SR_ERR_DEVICE_CHECK, "device bounds check failed");
+}
+
+static void fill_stats(sr_context *ctx, sr_stats *st) {
+  if (!st) return;
+  *st = ctx->prep_stats;
+  if (ctx->timing_valid) {
+    float k = 0.f, ev = 0.f, up = 0.f;
+    cudaEventElapsedTime(&k, ctx->ev[0], ctx->ev[3]);
+    cudaEventElapsedTime(&ev, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&up, ctx->ev[4], ctx->ev[5]);
+    st->gpu_kernel_time_ms = k;
+    st->eval_kernel_time_ms = ev;
+    st->data_transfer_time_ms = up;
+  }
+  if (ctx->mode == sr::Mode::kBatched || ctx->mode == sr::Mode::kCached) {
+    st->declared_sfu_ops = ctx->main.sfu_per_dp * static_cast<double>(ctx->N);
+    st->declared_fp32_ops = ctx->main.fp32_per_dp * static_cast<double>(ctx->N);
+  }
+  st->d2h_bytes += static_cast<int64_t>(ctx->E) * static_cast<int64_t>(sizeof(float)) +
+                   static_cast<int64_t>(sizeof(int32_t));
+  const sr::Plan &p = ctx->main.plan;
+  st->dpt = p.dpt;
+  st->warps_per_block = p.W;
+  st->blocks = p.blocks;
+  st->work_items = static_cast<int32_t>(p.items());
+}
+
+sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (ctx->E == 0) return SR_OK;
+  if (!mse_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "mse_out is NULL");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_mse.p, ctx->mse.p, ctx->E * sizeof(float),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  SR_TRY(check_device_error(ctx));
+  std::memcpy(mse_out, ctx->h_mse.p, ctx->E * sizeof(float));
+  fill_stats(ctx, stats);
+  return SR_OK;
+}
+
+sr_status sr_last_launch_times(sr_context *ctx, float *launch_ms, float *eval_kernel_ms) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (!ctx->timing_valid) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "no launch recorded");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+  float a = 0.f, b = 0.f;
+  SR_TRY_CUDA(ctx, cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[3]));
+  SR_TRY_CUDA(ctx, cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
+  if (launch_ms) *launch_ms = a;
+  if (eval_kernel_ms) *eval_kernel_ms = b;
+  return SR_OK;
+}
+
+sr_status sr_device_mse(sr_context *ctx, float **mse_dev) {
+  if (!ctx || !mse_dev) return SR_ERR_INVALID_ARGUMENT;
+  *mse_dev = ctx->mse.p;
+  return SR_OK;
+}
+
+sr_status sr_eval_mse(sr_context *ctx, const sr_population *pop, uint32_t flags, float *mse_out,
+                      sr_stats *stats) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  const double t0 = now_ms();
+  SR_TRY(sr_prepare(ctx, pop, flags));
+  if (pop->num_exprs == 0) {
+    if (stats) *stats = sr_stats{};
+    return SR_OK;
+  }
+  SR_TRY(sr_launch(ctx));
+  SR_TRY(sr_read_mse(ctx, mse_out, stats));
+  if (stats) stats->total_eval_time_ms = now_ms() - t0;
+  return SR_OK;
+}
+
+sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop, int64_t dp_begin,
+                              int64_t dp_count, float *pred_out) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  SR_TRY(check_population(ctx, pop));
+  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
+  if (dp_begin < 0 || dp_count < 0 || dp_begin + dp_count > ctx->N)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "datapoint range outside the dataset");
+  if (pop->num_exprs == 0 || dp_count == 0) return SR_OK;
+  if (!pred_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "pred_out is NULL");
+  const int E = pop->num_exprs;
+  const double bytes = static_cast<double>(E) * ctx->ldx * sizeof(float);
+  if (bytes > 16.0 * (1ull << 30))
+    return ctx->fail(SR_ERR_UNSUPPORTED, "prediction buffer would exceed 16 GiB");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->mode = sr::Mode::kNone;
+  SR_TRY(compile_set(ctx, E, pop->tokens, pop->values, pop->offsets, nullptr, ctx->main));
+  SR_TRY_CUDA(ctx, ctx->main.h_row.ensure(static_cast<size_t>(E)));
+  for (int x = 0; x < E; ++x) ctx->main.h_row.p[x] = x;
+  int dpt = ctx->opts.dpt ? ctx->opts.dpt : 8;
+  int W = ctx->opts.warps_per_block ? ctx->opts.warps_per_block : sr::kMaxWarps;
+  SR_TRY(plan_set(ctx, ctx->main, true, dpt, W));
+  SR_TRY(upload_code(ctx, ctx->main));
+  SR_TRY(upload_groups(ctx, ctx->main));
+  SR_TRY_CUDA(ctx, ctx->main.row.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->main.row.p, ctx->main.h_row.p, E * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+  SR_TRY_CUDA(ctx, ctx->pred.ensure(static_cast<size_t>(E) * ctx->ldx));
+  SR_TRY(launch_set(ctx, ctx->main, true, ctx->d_counter, ctx->pred.p, ctx->ldx, ctx->main.row.p));
+  SR_TRY_CUDA(ctx, cudaMemcpy2DAsync(pred_out, dp_count * sizeof(float), ctx->pred.p + dp_begin,
+                                     ctx->ldx * sizeof(float), dp_count * sizeof(float), E,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  SR_TRY(check_device_error(ctx));
+  return SR_OK;
+}
+
+sr_status sr_count_constants(const sr_population *pop, int64_t *const_offsets) {
+  if (!pop || !const_offsets || pop->num_exprs < 0) return SR_ERR_INVALID_ARGUMENT;
+  int64_t acc = 0;
+  for (int x = 0; x < pop->num_exprs; ++x) {
+    const_offsets[x] = acc;
+    for (int64_t i = pop->offsets[x]; i < pop->offsets[x + 1]; ++i)
+      acc += pop->tokens[i] == SR_TOK_CONST ? 1 : 0;
+  }
+  const_offsets[pop->num_exprs] = acc;
+  return SR_OK;
+}
+
+sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode, float *mse_out,
+                       float *grad_out, sr_stats *stats) {
+  (void)pop;
+  (void)mode;
+  (void)mse_out;
+  (void)grad_out;
+  (void)stats;
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  return ctx->fail(SR_ERR_UNSUPPORTED, "adjoint not built yet");
+}
+
+sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
+                                const sr_adam_options *adam, float *const_out, float *mse_out,
+                                sr_stats *stats) {
+  (void)pop;
+  (void)adam;
+  (void)const_out;
+  (void)mse_out;
+  (void)stats;
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  return ctx->fail(SR_ERR_UNSUPPORTED, "adjoint not built yet");
+}
+
+sr_status sr_get_stream(sr_context *ctx, void **stream) {
+  if (!ctx || !stream) return SR_ERR_INVALID_ARGUMENT;
+  *stream = ctx->stream;
+  return SR_OK;
+}
+
+sr_status sr_synchronize(sr_context *ctx) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SR_OK;
+}
+
+sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s, double *sfu_ops_per_s,
+                           int32_t *num_sms) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  DeviceScope scope(ctx->device);
+  float *dummy = nullptr;
+  SR_TRY_CUDA(ctx, cudaMalloc(&dummy, 1024 * sizeof(float)));
+  const int blocks = ctx->num_sms * 8, threads = 256, iters = 8192;
+  double rates[2] = {0, 0};
+  for (int m = 0; m < 2; ++m) {
+    const bool mufu = (m == 1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(ctx->ev[4], ctx->stream);
+      const cudaError_t e = sr::launch_pipe_bench(mufu, dummy, blocks, threads, iters, ctx->stream);
+      cudaEventRecord(ctx->ev[5], ctx->stream);
+      if (e != cudaSuccess || cudaEventSynchronize(ctx->ev[5]) != cudaSuccess) {
+        cudaFree(dummy);
+        return cuda_fail(ctx, e != cudaSuccess ? e : cudaGetLastError(), "pipe benchmark");
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+      if (rep > 0) best = std::min(best, ms);
+    }
+    rates[m] = static_cast<double>(blocks) * threads * iters * 8.0 / (best * 1e-3);
+  }
+  cudaFree(dummy);
+  if (fp32_ops_per_s) *fp32_ops_per_s = rates[0];
+  if (sfu_ops_per_s) *sfu_ops_per_s = rates[1];
+  if (num_sms) *num_sms = ctx->num_sms;
+  return SR_OK;
+}
+
+}  // extern "C"
+
+// ---- host-only helpers ------------------------------------------------------
+extern "C" {
+
+uint64_t sr_subtree_key(const int32_t *tokens, const double *values, int32_t len) {
+  if (!tokens || !values || len <= 0) return sr::kFnvOffset;
+  return sr::flat_key(tokens, values, len);
+}
+
+sr_status sr_subtree_hashes(const int32_t *tokens, const double *values, int32_t len,
+                            int32_t *sizes, uint64_t *hashes) {
+  if (!tokens || !values || !sizes || !hashes || len < 0) return SR_ERR_INVALID_ARGUMENT;
+  sr::merkle_hashes(tokens, values, len, sizes, hashes);
+  return SR_OK;
+}
+
+sr_status sr_detect_subtrees(const sr_population *pop, int32_t min_size, int32_t min_freq,
+                             int32_t max_groups, sr_detect_result *res, int32_t *group_expr,
+                             int32_t *group_pos, int32_t *group_size, int32_t *group_count,
+                             uint64_t *group_key) {
+  if (!pop || !res || pop->num_exprs < 0 || min_size < 1 || min_freq < 1)
+    return SR_ERR_INVALID_ARGUMENT;
+  if (pop->num_exprs > 0 && (!pop->tokens || !pop->values || !pop->offsets))
+    return SR_ERR_INVALID_ARGUMENT;
+  sr::Detection det;
+  sr::detect_common_subtrees(pop->num_exprs, pop->tokens, pop->values, pop->offsets, min_size,
+                             min_freq, static_cast<int>(std::thread::hardware_concurrency()), det);
+  res->num_subtrees = static_cast<int32_t>(det.groups.size());
+  res->total_tokens = det.total_tokens;
+  res->covered_tokens = det.covered_tokens;
+  res->avg_subtree_size = det.avg_subtree_size;
+  res->coverage = det.coverage;
+  const int n = std::min<int>(std::max(max_groups, 0), static_cast<int>(det.groups.size()));
+  for (int g = 0; g < n; ++g) {
+    const auto &G = det.groups[static_cast<size_t>(g)];
+    if (group_expr) group_expr[g] = G.expr;
+    if (group_pos) group_pos[g] = G.pos;
+    if (group_size) group_size[g] = G.size;
+    if (group_count) group_count[g] = G.occurrences;
+    if (group_key)
+      group_key[g] = sr::flat_key(pop->tokens + pop->offsets[G.expr] + G.pos,
+                                  pop->values + pop->offsets[G.expr] + G.pos, G.size);
+  }
+  return SR_OK;
+}
+
+sr_status sr_mark_cached(const sr_population *pop, const uint64_t *keys, const int32_t *slots,
+                         int32_t n_keys, int32_t *hints) {
+  if (!pop || pop->num_exprs < 0 || n_keys < 0 || (n_keys > 0 && (!keys || !slots)))
+    return SR_ERR_INVALID_ARGUMENT;
+  if (pop->num_exprs == 0) return SR_OK;
+  if (!pop->tokens || !pop->values || !pop->offsets || !hints) return SR_ERR_INVALID_ARGUMENT;
+  sr::SubtreeCache cache;
+  cache.capacity = n_keys;
+  for (int32_t k = 0; k < n_keys; ++k) cache.slot_of.emplace(keys[k], slots[k]);
+  cache.used = n_keys;
+  sr::mark_cached_subtrees(pop->num_exprs, pop->tokens, pop->values, pop->offsets, cache,
+                           static_cast<int>(std::thread::hardware_concurrency()), hints);
+  return SR_OK;
+}
+
+sr_status sr_validate_population(const sr_population *pop, int32_t num_vars, int32_t *n_instr,
+                                 int32_t *spill_slots, int32_t *bad_expr) {
+  if (bad_expr) *bad_expr = -1;
+  if (!pop || pop->num_exprs < 0 || num_vars < 0) return SR_ERR_INVALID_ARGUMENT;
+  if (pop->num_exprs == 0) return SR_OK;
+  if (!pop->tokens || !pop->values || !pop->offsets || pop->offsets[0] != 0)
+    return SR_ERR_INVALID_ARGUMENT;
+  std::vector<sr::Instr> scratch;
+  for (int x = 0; x < pop->num_exprs; ++x) {
+    const int64_t o = pop->offsets[x];
+    const int64_t len = pop->offsets[x + 1] - o;
+    sr::ExprInfo info;
+    sr_status s;
+    if (len <= 0) {
+      s = SR_ERR_MALFORMED_EXPRESSION;
+    } else if (len > SR_MAX_TOKENS) {
+      s = SR_ERR_EXPRESSION_TOO_LONG;
+    } else {
+      scratch.clear();
+      s = sr::compile_expression(pop->tokens + o, pop->values + o, static_cast<int>(len),
+                                 num_vars, nullptr, scratch, info, nullptr);
+    }
+    if (s != SR_OK) {
+      if (bad_expr) *bad_expr = x;
+      return s;
+    }
+    if (n_instr) n_instr[x] = info.n_instr;
+    if (spill_slots) spill_slots[x] = info.need;
+  }
+  return SR_OK;
+}
+
+}  // extern "C"

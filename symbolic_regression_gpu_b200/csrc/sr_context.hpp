@@ -1,0 +1,183 @@
+// sr_context.hpp — evaluator context: device-resident dataset, compiled
+// programs, launch plans and the subtree cache (reference
+// GPUSubtreeStateContext / SimpleGPUContext, src/cleaned/cl_gpu_common.h:26-212).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "sr_detect.hpp"
+#include "sr_eval.h"
+#include "sr_internal.hpp"
+#include "sr_program.hpp"
+
+namespace sr {
+
+// Grow-only device buffer.  Callers synchronise the stream before growing.
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (p && n <= cap) return cudaSuccess;
+    const size_t want = std::max<size_t>(n + n / 4, 64);
+    release();
+    const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    cap = want;
+    return cudaSuccess;
+  }
+};
+
+// Grow-only pinned host buffer used as the staging area of async copies.
+template <class T>
+struct PinnedBuf {
+  T *p = nullptr;
+  size_t cap = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf &) = delete;
+  PinnedBuf &operator=(const PinnedBuf &) = delete;
+  ~PinnedBuf() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+  cudaError_t ensure(size_t n) {
+    if (p && n <= cap) return cudaSuccess;
+    const size_t want = std::max<size_t>(n + n / 4, 64);
+    release();
+    const cudaError_t e = cudaMallocHost(&p, want * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    cap = want;
+    return cudaSuccess;
+  }
+};
+
+// Launch shape of one interpreter launch.
+struct Plan {
+  int dpt = 8;
+  int W = 8;
+  int smax = 0;
+  int n_groups = 0;
+  int n_spans = 0;
+  int tiles_per_span = 0;
+  int n_tiles = 0;
+  int blocks = 0;
+  size_t smem = 0;
+  int64_t items() const { return static_cast<int64_t>(n_groups) * n_spans; }
+};
+
+// A compiled population resident on the device.
+struct ProgramSet {
+  DevBuf<Instr> code;
+  DevBuf<int64_t> off;
+  DevBuf<int32_t> len;
+  DevBuf<int32_t> group;
+  DevBuf<int32_t> row;
+  PinnedBuf<Instr> h_code;
+  PinnedBuf<int64_t> h_off;
+  PinnedBuf<int32_t> h_len;
+  PinnedBuf<int32_t> h_group;
+  PinnedBuf<int32_t> h_row;
+  std::vector<float> cost;  // per expression
+  int E = 0;
+  int smax = 0;
+  int64_t n_instr = 0;
+  int64_t n_tokens = 0;      // tokens represented (skeleton-equivalent)
+  double sfu_per_dp = 0.0;   // declared work, summed over expressions
+  double fp32_per_dp = 0.0;
+  Plan plan;
+};
+
+// Buffers of the plain baseline kernel.
+struct PlainSet {
+  DevBuf<int32_t> tok;
+  DevBuf<float> val;
+  DevBuf<int64_t> off;
+  DevBuf<int32_t> len;
+  PinnedBuf<int32_t> h_tok;
+  PinnedBuf<float> h_val;
+  PinnedBuf<int64_t> h_off;
+  PinnedBuf<int32_t> h_len;
+  int E = 0;
+  int n_dpblocks = 0;
+};
+
+enum class Mode { kNone, kBatched, kCached, kPlain };
+
+}  // namespace sr
+
+struct sr_context {
+  sr_options opts{};
+  int device = 0;
+  int num_sms = 0;
+  std::string device_name;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+
+  // dataset
+  sr::DevBuf<float> X;
+  int64_t ldx = 0;
+  int32_t V = -1;
+  int64_t N = 0;
+
+  // compiled work
+  sr::ProgramSet main;   // expressions (or skeletons)
+  sr::ProgramSet sub;    // new cached subtrees of this call
+  sr::PlainSet plain;
+  sr::Mode mode = sr::Mode::kNone;
+  int E = 0;
+
+  // reduction / control
+  sr::DevBuf<double2> partial;
+  sr::DevBuf<float> mse;
+  sr::PinnedBuf<float> h_mse;
+  int32_t *d_counter = nullptr;   // [2]: main and subtree launches
+  int32_t *d_error = nullptr;
+  int32_t *h_error = nullptr;     // pinned
+
+  // subtree cache
+  sr::SubtreeCache cache;
+  sr::DevBuf<float> cache_vals;   // [capacity][ldx]
+  std::vector<int32_t> hints;     // per token of the last cached population
+
+  // predictions
+  sr::DevBuf<float> pred;
+
+  // timing
+  cudaEvent_t ev[6] = {};
+  bool timing_valid = false;
+
+  // statistics of the prepared population
+  sr_stats prep_stats{};
+
+  // tuned launch shapes: key -> (dpt, W)
+  std::map<std::string, std::pair<int, int>> tuned;
+  bool tune_loaded = false;
+
+  sr_status fail(sr_status s, const std::string &msg) {
+    last_error = msg;
+    return s;
+  }
+};

@@ -1,0 +1,31 @@
+// sr_kernels.hpp — host-callable launchers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "sr_internal.hpp"
+
+namespace sr {
+
+constexpr int kMaxWarps = 8;                        // evaluating warps per block
+constexpr int kMaxBlockThreads = (kMaxWarps + 1) * 32;  // + producer warp
+constexpr int kPlainStack = 128;                    // plain kernel stack depth
+
+// Dynamic shared memory of interp_kernel for a launch shape.
+size_t interp_smem_bytes(int dpt, int W, int V, int smax);
+// Sets the dynamic-smem attribute and returns resident blocks per SM.
+cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
+                             int *blocks_per_sm);
+cudaError_t launch_interp(int dpt, bool pred, const EvalArgs &args, int blocks,
+                          size_t smem, cudaStream_t stream);
+cudaError_t launch_finalize(const double2 *partial, int n_spans, int E,
+                            float *mse, cudaStream_t stream);
+cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *off,
+                         const int32_t *len, const float *X, int64_t ldx, int V,
+                         int64_t N, int E, double2 *partial, int n_dpblocks,
+                         cudaStream_t stream);
+cudaError_t launch_pipe_bench(bool mufu, float *out, int blocks, int threads,
+                              int iters, cudaStream_t stream);
+
+}  // namespace sr

@@ -1,0 +1,283 @@
+"""Python host API over the C ABI: the population evaluator.
+
+``Evaluator`` owns one ``sr_context``: a dataset resident on the GPU, the
+compiled population, and the cross-generation subtree cache.  Every call goes
+through libsr_eval.so; nothing here computes fitness itself.
+
+Reference counterparts: evaluate_gpu_mse_wrapper (src/cleaned/cl_gpu_eval.cu:578-592,
+subtree cache), evaluate_gpu_simple_wrapper (src/cleaned/cl_gpu_simple.cu:324-336).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .population import Population
+
+_F32P = ctypes.POINTER(ctypes.c_float)
+
+
+def _f32ptr(a: np.ndarray):
+    return a.ctypes.data_as(_F32P)
+
+
+class Evaluator:
+    """Population MSE evaluator on one GPU.
+
+    Parameters mirror ``sr_options`` (include/sr_eval.h).  ``stream`` may be a
+    ``torch.cuda.Stream`` (or a raw ``cudaStream_t`` integer); by default the
+    library creates its own stream.
+    """
+
+    def __init__(self, device: int = -1, *, cache_capacity: int = 2048,
+                 min_subtree_size: int = 3, min_subtree_freq: int = 10, dpt: int = 0,
+                 warps_per_block: int = 0, autotune: bool = False, host_threads: int = 0,
+                 tune_cache_path: Optional[str] = None, stream=None):
+        opts = _lib.sr_options()
+        _lib.check(_lib.lib.sr_options_init(ctypes.byref(opts)))
+        opts.device = device
+        opts.cache_capacity = cache_capacity
+        opts.min_subtree_size = min_subtree_size
+        opts.min_subtree_freq = min_subtree_freq
+        opts.dpt = dpt
+        opts.warps_per_block = warps_per_block
+        opts.autotune = 1 if autotune else 0
+        opts.host_threads = host_threads
+        self._tune_path = tune_cache_path.encode() if tune_cache_path else None
+        opts.tune_cache_path = self._tune_path
+        if stream is not None:
+            opts.stream = ctypes.c_void_p(getattr(stream, "cuda_stream", stream))
+        ctx = ctypes.c_void_p()
+        _lib.check(_lib.lib.sr_create(ctypes.byref(opts), ctypes.byref(ctx)), what="sr_create")
+        self._ctx = ctx
+        self.stats = _lib.sr_stats()
+        self.num_vars: Optional[int] = None
+        self.num_dps: Optional[int] = None
+        self._E = 0
+
+    # ---- lifecycle -----------------------------------------------------
+    def close(self):
+        if getattr(self, "_ctx", None):
+            _lib.lib.sr_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int, what: str):
+        _lib.check(status, self._ctx, what)
+
+    @property
+    def stream_handle(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(_lib.lib.sr_get_stream(self._ctx, ctypes.byref(s)), "sr_get_stream")
+        return s.value or 0
+
+    def synchronize(self):
+        self._check(_lib.lib.sr_synchronize(self._ctx), "sr_synchronize")
+
+    # ---- dataset -------------------------------------------------------
+    def set_data(self, X: np.ndarray):
+        """X: [(V+1), N] float32 rows (column-major dataset), y in the last row."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        if X.ndim != 2 or X.shape[0] < 1:
+            raise ValueError("X must be [(num_vars+1), num_dps]")
+        V, N = X.shape[0] - 1, X.shape[1]
+        self._check(_lib.lib.sr_set_data(self._ctx, _f32ptr(X), V, N), "sr_set_data")
+        self.num_vars, self.num_dps = V, N
+
+    def set_data_device(self, X, ld: Optional[int] = None):
+        """X: a CUDA tensor [(V+1), N] float32 (row stride ld, default N)."""
+        V, N = int(X.shape[0]) - 1, int(X.shape[1])
+        ld = int(X.stride(0)) if ld is None else ld
+        self._check(_lib.lib.sr_set_data_device(self._ctx, ctypes.c_void_p(X.data_ptr()), ld, V, N),
+                    "sr_set_data_device")
+        self.num_vars, self.num_dps = V, N
+
+    # ---- evaluation ----------------------------------------------------
+    @staticmethod
+    def _flags(cache: bool, clear_cache: bool, plain: bool) -> int:
+        f = 0
+        if cache:
+            f |= _lib.SR_EVAL_SUBTREE_CACHE
+        if clear_cache:
+            f |= _lib.SR_EVAL_CLEAR_CACHE
+        if plain:
+            f |= _lib.SR_EVAL_PLAIN
+        return f
+
+    def eval_mse(self, pop: Population, *, cache: bool = False, clear_cache: bool = False,
+                 plain: bool = False) -> np.ndarray:
+        """Per-expression MSE (float32 [E]); NaN where no datapoint is valid."""
+        out = np.empty(pop.num_exprs, np.float32)
+        cpop = pop.as_c()
+        self._check(_lib.lib.sr_eval_mse(self._ctx, ctypes.byref(cpop),
+                                         self._flags(cache, clear_cache, plain), _f32ptr(out),
+                                         ctypes.byref(self.stats)), "sr_eval_mse")
+        return out
+
+    def prepare(self, pop: Population, *, cache: bool = False, clear_cache: bool = False,
+                plain: bool = False):
+        cpop = pop.as_c()
+        self._check(_lib.lib.sr_prepare(self._ctx, ctypes.byref(cpop),
+                                        self._flags(cache, clear_cache, plain)), "sr_prepare")
+        self._E = pop.num_exprs
+
+    def launch(self):
+        """Enqueue the prepared evaluation on the context stream (asynchronous)."""
+        self._check(_lib.lib.sr_launch(self._ctx), "sr_launch")
+
+    def read_mse(self) -> np.ndarray:
+        out = np.empty(self._E, np.float32)
+        self._check(_lib.lib.sr_read_mse(self._ctx, _f32ptr(out), ctypes.byref(self.stats)),
+                    "sr_read_mse")
+        return out
+
+    def last_launch_times(self):
+        """(whole launch ms, main interpreter kernel ms) of the last launch."""
+        a = ctypes.c_float()
+        b = ctypes.c_float()
+        self._check(_lib.lib.sr_last_launch_times(self._ctx, ctypes.byref(a), ctypes.byref(b)),
+                    "sr_last_launch_times")
+        return a.value, b.value
+
+    def device_mse_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(_lib.lib.sr_device_mse(self._ctx, ctypes.byref(p)), "sr_device_mse")
+        return p.value or 0
+
+    def predictions(self, pop: Population, dp_begin: int = 0,
+                    dp_count: Optional[int] = None) -> np.ndarray:
+        """Raw FP32 predictions [E, dp_count] (NaN/Inf included)."""
+        if dp_count is None:
+            dp_count = (self.num_dps or 0) - dp_begin
+        out = np.empty((pop.num_exprs, dp_count), np.float32)
+        cpop = pop.as_c()
+        self._check(_lib.lib.sr_eval_predictions(self._ctx, ctypes.byref(cpop), dp_begin,
+                                                 dp_count, _f32ptr(out)), "sr_eval_predictions")
+        return out
+
+    def eval_grad(self, pop: Population, mode: int = _lib.SR_GRAD_RECOMPUTE):
+        """(mse [E], d mse / d constants [C]) with constants in token order."""
+        nconst = int(np.count_nonzero(pop.tokens == 0))
+        mse = np.empty(pop.num_exprs, np.float32)
+        grad = np.empty(max(nconst, 1), np.float32)
+        cpop = pop.as_c()
+        self._check(_lib.lib.sr_eval_grad(self._ctx, ctypes.byref(cpop), mode, _f32ptr(mse),
+                                          _f32ptr(grad), ctypes.byref(self.stats)),
+                    "sr_eval_grad")
+        return mse, grad[:nconst]
+
+    def optimize_constants(self, pop: Population, steps: int = 20, lr: float = 0.05,
+                           beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8,
+                           mode: int = _lib.SR_GRAD_RECOMPUTE):
+        """On-device Adam over every expression's constants.
+        Returns (constants [C] after `steps`, mse [E] at those constants)."""
+        nconst = int(np.count_nonzero(pop.tokens == 0))
+        adam = _lib.sr_adam_options(steps, mode, lr, beta1, beta2, eps)
+        consts = np.empty(max(nconst, 1), np.float32)
+        mse = np.empty(pop.num_exprs, np.float32)
+        cpop = pop.as_c()
+        self._check(_lib.lib.sr_optimize_constants(self._ctx, ctypes.byref(cpop),
+                                                   ctypes.byref(adam), _f32ptr(consts),
+                                                   _f32ptr(mse), ctypes.byref(self.stats)),
+                    "sr_optimize_constants")
+        return consts[:nconst], mse
+
+    def measure_pipes(self):
+        """(FP32 FMA ops/s, MUFU ops/s, SM count) measured on this device."""
+        f = ctypes.c_double()
+        s = ctypes.c_double()
+        n = ctypes.c_int32()
+        self._check(_lib.lib.sr_measure_pipes(self._ctx, ctypes.byref(f), ctypes.byref(s),
+                                              ctypes.byref(n)), "sr_measure_pipes")
+        return f.value, s.value, n.value
+
+
+# ---- host-only helpers (no GPU needed) ------------------------------------
+
+def subtree_key(tokens, values) -> int:
+    """Flat cache key of a token/value run (reference compute_subtree_hash_gpu,
+    src/cleaned/cl_gpu_eval.cu:259-272)."""
+    t = np.ascontiguousarray(tokens, np.int32)
+    v = np.ascontiguousarray(values, np.float64)
+    return int(_lib.lib.sr_subtree_key(t.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                       v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), t.size))
+
+
+def subtree_hashes(tokens, values):
+    """(sizes int32 [L], Merkle hashes uint64 [L]) of one expression
+    (reference detect.cpp:169-191)."""
+    t = np.ascontiguousarray(tokens, np.int32)
+    v = np.ascontiguousarray(values, np.float64)
+    sizes = np.empty(t.size, np.int32)
+    hashes = np.empty(t.size, np.uint64)
+    _lib.check(_lib.lib.sr_subtree_hashes(
+        t.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+        v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), t.size,
+        sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+        hashes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+    return sizes, hashes
+
+
+def detect_subtrees(pop: Population, min_size: int = 3, min_freq: int = 10):
+    """Common-subtree detection (reference detect_common_subtrees,
+    src/utils/detect.cpp:120-387).  Returns (stats dict, groups dict of arrays)."""
+    res = _lib.sr_detect_result()
+    cpop = pop.as_c()
+    _lib.check(_lib.lib.sr_detect_subtrees(ctypes.byref(cpop), min_size, min_freq, 0,
+                                           ctypes.byref(res), None, None, None, None, None))
+    n = res.num_subtrees
+    ge = np.empty(max(n, 1), np.int32)
+    gp = np.empty(max(n, 1), np.int32)
+    gs = np.empty(max(n, 1), np.int32)
+    gc = np.empty(max(n, 1), np.int32)
+    gk = np.empty(max(n, 1), np.uint64)
+    P = ctypes.POINTER
+    _lib.check(_lib.lib.sr_detect_subtrees(
+        ctypes.byref(cpop), min_size, min_freq, n, ctypes.byref(res),
+        ge.ctypes.data_as(P(ctypes.c_int32)), gp.ctypes.data_as(P(ctypes.c_int32)),
+        gs.ctypes.data_as(P(ctypes.c_int32)), gc.ctypes.data_as(P(ctypes.c_int32)),
+        gk.ctypes.data_as(P(ctypes.c_uint64))))
+    stats = {f: getattr(res, f) for f, _ in res._fields_ if f != "reserved0"}
+    groups = {"expr": ge[:n], "pos": gp[:n], "size": gs[:n], "count": gc[:n], "key": gk[:n]}
+    return stats, groups
+
+
+def mark_cached(pop: Population, keys, slots) -> np.ndarray:
+    """Cache-marking hints per token (reference mark_cached_subtrees_from_state,
+    src/cleaned/cl_gpu_eval.cu:294-329)."""
+    k = np.ascontiguousarray(keys, np.uint64)
+    s = np.ascontiguousarray(slots, np.int32)
+    hints = np.empty(max(pop.num_tokens, 1), np.int32)
+    cpop = pop.as_c()
+    P = ctypes.POINTER
+    _lib.check(_lib.lib.sr_mark_cached(ctypes.byref(cpop), k.ctypes.data_as(P(ctypes.c_uint64)),
+                                       s.ctypes.data_as(P(ctypes.c_int32)), k.size,
+                                       hints.ctypes.data_as(P(ctypes.c_int32))))
+    return hints[:pop.num_tokens]
+
+
+def validate(pop: Population, num_vars: int):
+    """(n_instr [E], spill_slots [E]); raises SrError naming the bad expression."""
+    n_instr = np.empty(max(pop.num_exprs, 1), np.int32)
+    slots = np.empty(max(pop.num_exprs, 1), np.int32)
+    bad = ctypes.c_int32(-1)
+    cpop = pop.as_c()
+    P = ctypes.POINTER
+    st = _lib.lib.sr_validate_population(ctypes.byref(cpop), num_vars,
+                                         n_instr.ctypes.data_as(P(ctypes.c_int32)),
+                                         slots.ctypes.data_as(P(ctypes.c_int32)),
+                                         ctypes.byref(bad))
+    if st != _lib.SR_OK:
+        raise _lib.SrError(st, f"expression {bad.value}: {_lib.status_string(st)}")
+    return n_instr[:pop.num_exprs], slots[:pop.num_exprs]

@@ -1,0 +1,73 @@
+"""The C-ABI library loads and exports every symbol its headers declare."""
+import ctypes
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+LIB = os.path.join(ROOT, "symbolic_regression_gpu_b200", "lib", "libsr_eval.so")
+
+
+def _declared_c_functions():
+    src = open(os.path.join(ROOT, "include", "sr_eval.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(sr_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_c_symbol():
+    lib = ctypes.CDLL(LIB)
+    names = _declared_c_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_declares_every_c_symbol():
+    from symbolic_regression_gpu_b200 import _lib
+    assert set(_declared_c_functions()) <= set(_lib._SIGNATURES)
+
+
+@pytest.mark.skipif(shutil.which("nm") is None, reason="nm not available")
+def test_reference_cpp_entry_points_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", "-C", LIB], capture_output=True,
+                         text=True, check=True).stdout
+    for sig in [
+        "create_gpu_context()",
+        "destroy_gpu_context(void*)",
+        "evaluate_gpu_mse_wrapper(InputInfo&, float***, std::vector<float, "
+        "std::allocator<float> >&, void*, bool, bool, RunStats&)",
+        "create_gpu_simple_context()",
+        "destroy_gpu_simple_context(void*)",
+        "evaluate_gpu_simple_wrapper(InputInfo&, float***, std::vector<float, "
+        "std::allocator<float> >&, void*, bool, RunStats&)",
+    ]:
+        assert sig in out, sig
+
+
+def test_abi_version_and_status_strings():
+    from symbolic_regression_gpu_b200 import _lib
+    assert _lib.lib.sr_abi_version() == 1
+    for s in range(13):
+        assert _lib.status_string(s) not in ("", "unknown status")
+
+
+def test_create_without_device_reports_status():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from symbolic_regression_gpu_b200 import Evaluator, SrError, _lib
+    with pytest.raises(SrError) as ei:
+        Evaluator()
+    assert ei.value.status == _lib.SR_ERR_NO_DEVICE
+
+
+def test_null_arguments_are_rejected():
+    from symbolic_regression_gpu_b200 import _lib
+    assert _lib.lib.sr_create(None, None) == _lib.SR_ERR_INVALID_ARGUMENT
+    assert _lib.lib.sr_options_init(None) == _lib.SR_ERR_INVALID_ARGUMENT
+    assert _lib.lib.sr_destroy(None) == _lib.SR_OK
+    assert _lib.lib.sr_launch(None) == _lib.SR_ERR_INVALID_ARGUMENT

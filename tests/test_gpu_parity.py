@@ -1,0 +1,257 @@
+"""CUDA path against the reference's outputs (golden vectors) and the oracle.
+
+Tolerances (stated once, used below):
+  * IEEE operations (+ - * / sqrt, reciprocal, min/max, abs, neg, protected
+    variants): bit-identical predictions.
+  * Transcendental operators: CUDA's sinf/expf/... against glibc's: <= 4 ulp
+    per datapoint for single-operator expressions on finite results.
+  * MSE against the reference CPU evaluator: <= 1e-6 relative where the
+    per-datapoint predictions are bit-identical (IEEE-only expressions), and the
+    distribution otherwise (median <= 1e-7, 99th percentile <= 1e-5).
+  * Reduction error (GPU MSE vs FP64 sum of the GPU's own FP32 predictions):
+    <= 2e-7 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import oracle
+import symbolic_regression_gpu_b200 as sg
+from symbolic_regression_gpu_b200 import opcodes as op
+from symbolic_regression_gpu_b200 import synth
+from symbolic_regression_gpu_b200.population import Population
+
+pytestmark = pytest.mark.gpu
+
+IEEE_OPS = {op.ADD, op.SUB, op.MUL, op.DIV, op.MIN, op.MAX, op.LOOSE_DIV, op.INV,
+            op.LOOSE_INV, op.ABS, op.NEG, op.SQRT, op.LOOSE_SQRT}
+
+
+def ordered(x):
+    i = np.asarray(x, np.float32).view(np.int32).astype(np.int64)
+    return np.where(i < 0, -(i & 0x7FFFFFFF), i)
+
+
+def ulp(a, b):
+    return np.abs(ordered(a) - ordered(b))
+
+
+def same_float(a, b):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    return (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.abs(a - b) / np.maximum(np.abs(b), 1e-30)
+
+
+def ieee_only(pop):
+    return np.array([set(t[t > 0].tolist()) <= IEEE_OPS for t, _ in pop])
+
+
+def test_single_operator_predictions(evaluator):
+    pop, d = load_golden("eval_all_ops.npz")
+    n_edge = 31
+    edge = pop.slice(0, n_edge)
+    evaluator.set_data(d["X"])
+    pred = evaluator.predictions(edge)
+    ref = d["pred"][:n_edge]
+    for i, (t, _) in enumerate(edge):
+        ops = set(t[t > 0].tolist())
+        nan_g, nan_r = np.isnan(pred[i]), np.isnan(ref[i])
+        assert (nan_g == nan_r).all(), f"expr {i} {t}: NaN pattern differs"
+        fin = np.isfinite(ref[i]) & np.isfinite(pred[i])
+        assert (np.isinf(pred[i]) == np.isinf(ref[i])).all(), f"expr {i}: Inf pattern differs"
+        if ops <= IEEE_OPS:
+            assert same_float(pred[i], ref[i]).all(), f"expr {i} {t}: not bit-identical"
+        else:
+            worst = int(ulp(pred[i][fin], ref[i][fin]).max(initial=0))
+            assert worst <= 4, f"expr {i} {t}: {worst} ulp"
+
+
+def test_random_all_ops_predictions(evaluator):
+    pop, d = load_golden("eval_all_ops.npz")
+    evaluator.set_data(d["X"])
+    pred = evaluator.predictions(pop)
+    ref = d["pred"]
+    nan_agree = (np.isnan(pred) == np.isnan(ref)).mean()
+    assert nan_agree >= 0.995, nan_agree
+    fin = np.isfinite(pred) & np.isfinite(ref)
+    u = ulp(pred[fin], ref[fin])
+    assert (u <= 4).mean() >= 0.99, f"{(u <= 4).mean():.4f} of datapoints within 4 ulp"
+    ieee = ieee_only(pop)
+    assert same_float(pred[ieee], ref[ieee]).all()
+
+
+def test_workload_ops_predictions_vs_oracle(evaluator):
+    w = synth.plain_workload(seed=11, E=200, N=4096)
+    evaluator.set_data(w.X)
+    pred = evaluator.predictions(w.population)
+    ref = oracle.predict_f32(w.population, w.X)
+    assert (np.isnan(pred) == np.isnan(ref)).mean() >= 0.999
+    fin = np.isfinite(pred) & np.isfinite(ref)
+    u = ulp(pred[fin], ref[fin])
+    assert (u <= 4).mean() >= 0.99, f"{(u <= 4).mean():.4f} within 4 ulp"
+
+
+def test_mse_vs_reference_golden(evaluator):
+    pop, d = load_golden("eval_workload_ops.npz")
+    evaluator.set_data(d["X"])
+    mse = evaluator.eval_mse(pop)
+    ref = d["mse"]
+    assert (np.isnan(mse) == np.isnan(ref)).all()
+    ok = np.isfinite(ref)
+    r = rel(mse[ok], ref[ok])
+    assert np.median(r) <= 1e-7, np.median(r)
+    assert np.quantile(r, 0.99) <= 1e-5, np.quantile(r, 0.99)
+    ieee = ieee_only(pop) & ok
+    assert (rel(mse[ieee], ref[ieee]) <= 1e-6).all()
+
+
+def test_mse_all_ops_vs_reference_golden(evaluator):
+    pop, d = load_golden("eval_all_ops.npz")
+    evaluator.set_data(d["X"])
+    mse = evaluator.eval_mse(pop)
+    ref = d["mse"]
+    assert (np.isnan(mse) == np.isnan(ref)).all()
+    assert (np.isinf(mse) == np.isinf(ref)).all()
+    ieee = ieee_only(pop) & np.isfinite(ref)
+    assert (rel(mse[ieee], ref[ieee]) <= 1e-6).all()
+
+
+def test_reduction_error(evaluator):
+    w = synth.plain_workload(seed=12, E=120, N=50_000)
+    evaluator.set_data(w.X)
+    pred = evaluator.predictions(w.population)
+    mse = evaluator.eval_mse(w.population)
+    want = oracle.mse_of_predictions(pred, w.X[-1])
+    assert (np.isnan(mse) == np.isnan(want)).all()
+    ok = np.isfinite(want)
+    assert (rel(mse[ok], want[ok]) <= 2e-7).all(), rel(mse[ok], want[ok]).max()
+
+
+def test_mse_vs_fp64_oracle(evaluator):
+    w = synth.plain_workload(seed=13, E=200, N=20_000)
+    evaluator.set_data(w.X)
+    mse = evaluator.eval_mse(w.population)
+    m64, cnt = oracle.mse_f64(w.population, w.X)
+    ok = np.isfinite(m64) & np.isfinite(mse) & (cnt == w.num_dps)
+    r = rel(mse[ok], m64[ok])
+    assert np.median(r) <= 1e-5, np.median(r)
+
+
+@pytest.mark.parametrize("dpt,warps", [(4, 1), (4, 8), (8, 3), (8, 8)])
+def test_launch_shapes_agree(dpt, warps):
+    w = synth.plain_workload(seed=14, E=77, N=3001)
+    ref = oracle.mse_f32(w.population, w.X)
+    with sg.Evaluator(device=0, dpt=dpt, warps_per_block=warps) as ev:
+        ev.set_data(w.X)
+        mse = ev.eval_mse(w.population)
+        pred = ev.predictions(w.population)
+    base = oracle.predict_f32(w.population, w.X)
+    ieee = ieee_only(w.population)
+    assert same_float(pred[ieee], base[ieee]).all()
+    ok = np.isfinite(ref)
+    assert (np.isnan(mse) == np.isnan(ref)).all()
+    assert np.median(rel(mse[ok], ref[ok])) <= 1e-7
+
+
+def test_plain_kernel_matches_batched(evaluator):
+    w = synth.plain_workload(seed=15, E=150, N=10_000)
+    evaluator.set_data(w.X)
+    a = evaluator.eval_mse(w.population)
+    b = evaluator.eval_mse(w.population, plain=True)
+    assert (np.isnan(a) == np.isnan(b)).all()
+    ok = np.isfinite(a)
+    assert (rel(a[ok], b[ok]) <= 1e-6).all()
+
+
+@pytest.mark.parametrize("N", [1, 2, 127, 255, 256, 257, 1023, 1025, 4097])
+def test_ragged_sizes(evaluator, N):
+    w = synth.plain_workload(seed=16, E=37, N=N)
+    evaluator.set_data(w.X)
+    mse = evaluator.eval_mse(w.population)
+    ref = oracle.mse_f32(w.population, w.X)
+    assert (np.isnan(mse) == np.isnan(ref)).all()
+    ok = np.isfinite(ref)
+    assert (rel(mse[ok], ref[ok]) <= 1e-5).all()
+    pred = evaluator.predictions(w.population)
+    assert pred.shape == (37, N)
+
+
+def test_zero_datapoints_gives_nan(evaluator):
+    X = np.zeros((3, 0), np.float32)
+    evaluator.set_data(X)
+    pop = Population.from_lists([([op.ADD, -1, 0], [0, 0, 1.0])])
+    assert np.isnan(evaluator.eval_mse(pop)).all()
+
+
+def test_empty_population(evaluator):
+    w = synth.plain_workload(seed=17, E=3, N=100)
+    evaluator.set_data(w.X)
+    empty = Population(np.zeros(0, np.int32), np.zeros(0), np.zeros(1, np.int64))
+    assert evaluator.eval_mse(empty).shape == (0,)
+
+
+def test_longest_expression_and_extreme_var_counts(evaluator):
+    import sys
+    sys.setrecursionlimit(max(sys.getrecursionlimit(), 10_000))
+    rng = np.random.default_rng(18)
+    for V in (0, 1, 31):
+        N = 700
+        X = rng.uniform(-2, 2, size=(V + 1, N)).astype(np.float32)
+        gen = synth.TreeGen(rng, V)
+        exprs = [gen.sized_tree(1000), gen.sized_tree(1), gen.sized_tree(3)]
+        # a deep left-leaning chain: raw stack depth 1 but 1023 tokens
+        t = [op.ADD] * 511 + [op.TOK_CONST] * 512
+        exprs.append((t, [0.0] * 511 + list(rng.uniform(-1, 1, 512))))
+        pop = Population.from_lists(exprs)
+        evaluator.set_data(X)
+        mse = evaluator.eval_mse(pop)
+        ref = oracle.mse_f32(pop, X)
+        assert (np.isnan(mse) == np.isnan(ref)).all()
+        ok = np.isfinite(ref)
+        assert (rel(mse[ok], ref[ok]) <= 1e-4).all(), (V, mse, ref)
+
+
+def test_invalid_datapoints_masked(evaluator):
+    X = np.array([[0.0, 1.0, -1.0, 2.0], [0.0, 0.0, 0.0, 0.0]], np.float32)
+    evaluator.set_data(X)
+    pop = Population.from_lists([
+        ([op.DIV, op.TOK_CONST, op.TOK_VAR], [0, 1.0, 0]),    # 1/x: NaN? no: Inf at x=0
+        ([op.LOG, op.TOK_VAR], [0, 0]),                       # NaN for x<0, -Inf at 0
+        ([op.DIV, op.TOK_VAR, op.TOK_CONST], [0, 0, 0.0]),    # always NaN
+        ([op.MUL, op.TOK_CONST, op.TOK_VAR], [0, 3e19, 0]),   # square overflows -> Inf
+    ])
+    mse = evaluator.eval_mse(pop)
+    ref = oracle.mse_f32(pop, X)
+    assert same_float(mse, ref).all(), (mse, ref)
+    assert np.isnan(mse[2]) and np.isinf(mse[3])
+
+
+def test_prepare_launch_read_is_repeatable(evaluator):
+    w = synth.plain_workload(seed=19, E=64, N=20_000)
+    evaluator.set_data(w.X)
+    evaluator.prepare(w.population)
+    outs = []
+    for _ in range(3):
+        evaluator.launch()
+        outs.append(evaluator.read_mse())
+    assert same_float(outs[0], outs[1]).all() and same_float(outs[1], outs[2]).all()
+    assert evaluator.stats.kernel_launches >= 2
+    assert evaluator.stats.node_evals == w.population.num_tokens * w.num_dps
+
+
+def test_bad_input_reports_status(evaluator):
+    w = synth.plain_workload(seed=20, E=4, N=100)
+    evaluator.set_data(w.X)
+    bad = Population.from_lists([([op.ADD, -1], [0, 0])])
+    with pytest.raises(sg.SrError) as ei:
+        evaluator.eval_mse(bad)
+    assert ei.value.status == sg._lib.SR_ERR_MALFORMED_EXPRESSION
+    # the context stays usable
+    assert np.isfinite(evaluator.eval_mse(w.population)).any()
