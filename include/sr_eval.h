@@ -284,6 +284,24 @@ sr_status sr_mark_cached(const sr_population *pop, const uint64_t *keys, const i
 sr_status sr_validate_population(const sr_population *pop, int32_t num_vars,
                                  int32_t *n_instr, int32_t *spill_slots, int32_t *bad_expr);
 
+/* The interpreter bytecode of a population, as sr_prepare compiles it (for
+ * inspection and host-side verification of the compiler).  Each instruction
+ * is 4 uint32 words {w, a, b, c} and executes
+ *     [spill T -> S[slot]]  [T = leaf a]  [b = operand b]  T = op(T, b):
+ *   w bits 0..5 opcode: reference token 1..9 (T = f(T, b)), 10..27 (T = f(T)),
+ *     32 = exp clamped at 80, 40 + k = reversed binary k (T = f_k(b, T)),
+ *     0 = none; bit 6 load leaf a into T, bits 7..8 its kind (0 = variable,
+ *     1 = constant, 2 = cached subtree); bits 9..11 kind of operand b
+ *     (0 = none, 1 = spill slot, 2 = variable, 3 = constant, 4 = cached
+ *     subtree); bit 12 spill T into slot bits 13..17 first;
+ *   a, b payloads (variable index / float bits / slot);
+ *   c bits 0..9 / 10..19 constant index of leaf a / operand b (0x3FF = none).
+ * code may be NULL to query sizes: instr_offsets (num_exprs+1) always
+ * receives the per-expression instruction offsets. */
+sr_status sr_compile_population(const sr_population *pop, int32_t num_vars, uint32_t *code,
+                                int64_t code_capacity, int64_t *instr_offsets,
+                                int32_t *spill_slots);
+
 /* ---- misc ------------------------------------------------------------------ */
 sr_status sr_get_stream(sr_context *ctx, void **stream);
 sr_status sr_synchronize(sr_context *ctx);

@@ -11,7 +11,10 @@ import os
 from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int32,
                     c_int64, c_uint32, c_uint64, c_void_p)
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libsr_eval.so")
+# SR_EVAL_LIBRARY selects another build of the library explicitly (a path that
+# does not exist fails the import like a missing default build).
+LIB_PATH = os.environ.get("SR_EVAL_LIBRARY") or os.path.join(
+    os.path.dirname(os.path.abspath(__file__)), "lib", "libsr_eval.so")
 
 # status codes (sr_status)
 SR_OK = 0
@@ -149,6 +152,8 @@ _SIGNATURES = {
                                  _P(c_int32)]),
     "sr_validate_population": (c_int32, [_P(sr_population), c_int32, _P(c_int32), _P(c_int32),
                                          _P(c_int32)]),
+    "sr_compile_population": (c_int32, [_P(sr_population), c_int32, _P(c_uint32), c_int64,
+                                        _P(c_int64), _P(c_int32)]),
     "sr_get_stream": (c_int32, [c_void_p, _P(c_void_p)]),
     "sr_synchronize": (c_int32, [c_void_p]),
     "sr_measure_pipes": (c_int32, [c_void_p, _P(c_double), _P(c_double), _P(c_int32)]),

@@ -156,60 +156,54 @@ sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *
   return SR_OK;
 }
 
-// Launch shape: groups of W cost-sorted expressions x spans of tiles.
-sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W) {
+// Launch shape: groups of G cost-sorted expressions x spans of datapoints.
+sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
+                   int span_target = 1024, int per_warp = 4) {
   sr::Plan p;
   p.dpt = dpt;
   p.W = W;
   p.smax = std::max(ps.smax, 0);
   const int64_t tile = 32 * dpt;
   const int E = ps.E;
-  p.n_tiles = static_cast<int>((ctx->N + tile - 1) / tile);
-  p.n_groups = (E + W - 1) / W;
-  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.smax);
+  p.G = std::max(1, W * per_warp);
+  p.n_groups = (E + p.G - 1) / p.G;
   int dev_max_smem = 0;
   cudaDeviceGetAttribute(&dev_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+  // Span: the target, shrunk to the data and to the shared-memory budget.
+  int64_t span = std::min<int64_t>(span_target, std::max<int64_t>(tile, round_up(ctx->N, tile)));
+  while (span > tile &&
+         sr::interp_smem_bytes(dpt, W, ctx->V, p.smax, static_cast<int>(span)) >
+             static_cast<size_t>(dev_max_smem))
+    span = std::max<int64_t>(tile, span / 2);
+  p.span = static_cast<int>(span);
+  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.smax, p.span);
   if (p.smem > static_cast<size_t>(dev_max_smem))
     return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape needs " + std::to_string(p.smem) +
                                              " bytes of shared memory");
+  p.n_spans = (ctx->N == 0 || E == 0) ? 0 : static_cast<int>((ctx->N + span - 1) / span);
+  if (!pred && static_cast<double>(p.n_spans) * E * 16.0 > 8.0 * (1ull << 30))
+    return ctx->fail(SR_ERR_UNSUPPORTED, "partial-sum buffer would exceed 8 GiB");
   int bps = 0;
   SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.smem, W, &bps));
   if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
   const int64_t resident = static_cast<int64_t>(bps) * ctx->num_sms;
-  if (p.n_tiles == 0 || E == 0) {
-    p.n_spans = 0;
-    p.tiles_per_span = 0;
-  } else {
-    const int64_t target = 8 * resident;
-    int64_t spans = (target + p.n_groups - 1) / p.n_groups;
-    spans = std::max<int64_t>(1, std::min<int64_t>(spans, p.n_tiles));
-    if (!pred) {
-      const int64_t cap = std::max<int64_t>(1, (int64_t{1} << 28) / (16 * static_cast<int64_t>(E)));
-      spans = std::min(spans, cap);
-    }
-    // Per-warp datapoint counts stay below 2^30 (int counters).
-    const int64_t min_spans = (static_cast<int64_t>(p.n_tiles) * tile + (int64_t{1} << 30) - 1) >> 30;
-    spans = std::max(spans, min_spans);
-    const int64_t tps = (p.n_tiles + spans - 1) / spans;
-    p.tiles_per_span = static_cast<int>(tps);
-    p.n_spans = static_cast<int>((p.n_tiles + tps - 1) / tps);
-  }
   p.blocks = static_cast<int>(std::min<int64_t>(resident, std::max<int64_t>(p.items(), 1)));
-  // Group table: expressions in decreasing modelled cost, W per group.
-  SR_TRY_CUDA(ctx, ps.h_group.ensure(static_cast<size_t>(std::max(p.n_groups * W, 1))));
+  // Group table: expressions in decreasing modelled cost, G per group, so
+  // every group holds similar work and hands out its largest first.
+  SR_TRY_CUDA(ctx, ps.h_group.ensure(static_cast<size_t>(std::max(p.n_groups * p.G, 1))));
   std::vector<int32_t> order(static_cast<size_t>(E));
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
     return ps.cost[static_cast<size_t>(a)] > ps.cost[static_cast<size_t>(b)];
   });
-  for (int64_t k = 0; k < static_cast<int64_t>(p.n_groups) * W; ++k)
+  for (int64_t k = 0; k < static_cast<int64_t>(p.n_groups) * p.G; ++k)
     ps.h_group.p[k] = k < E ? order[static_cast<size_t>(k)] : -1;
   ps.plan = p;
   return SR_OK;
 }
 
 sr_status upload_groups(sr_context *ctx, ProgramSet &ps) {
-  const size_t ng = static_cast<size_t>(std::max(ps.plan.n_groups * ps.plan.W, 1));
+  const size_t ng = static_cast<size_t>(std::max(ps.plan.n_groups * ps.plan.G, 1));
   ctx->prep_stats.h2d_bytes += static_cast<int64_t>(ng * sizeof(int32_t));
   SR_TRY_CUDA(ctx, ps.group.ensure(ng));
   SR_TRY_CUDA(ctx, cudaMemcpyAsync(ps.group.p, ps.h_group.p, ng * sizeof(int32_t),
@@ -253,10 +247,10 @@ sr::EvalArgs make_args(sr_context *ctx, ProgramSet &ps, int32_t *counter) {
   a.E = ps.E;
   a.W = ps.plan.W;
   a.smax = ps.plan.smax;
+  a.G = ps.plan.G;
   a.n_groups = ps.plan.n_groups;
+  a.span = ps.plan.span;
   a.n_spans = ps.plan.n_spans;
-  a.tiles_per_span = ps.plan.tiles_per_span;
-  a.n_tiles = ps.plan.n_tiles;
   return a;
 }
 
@@ -320,7 +314,7 @@ void save_tune_cache(const sr_context *ctx) {
 
 // Times each candidate shape on the prepared population and keeps the fastest.
 sr_status autotune_main(sr_context *ctx, const std::string &key) {
-  static const int kCand[][2] = {{8, 8}, {8, 6}, {8, 4}, {4, 8}, {4, 4}};
+  static const int kCand[][2] = {{8, 8}, {8, 12}, {8, 16}, {4, 8}, {4, 16}};
   float best = 1e30f;
   int best_dpt = 8, best_w = 8;
   cudaEvent_t a = ctx->ev[4], b = ctx->ev[5];
@@ -494,7 +488,7 @@ sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, in
                                                " exceeds " + std::to_string(SR_MAX_VARS));
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  const int64_t ldx = std::max<int64_t>(1024, round_up(num_dps, 1024));
+  const int64_t ldx = std::max<int64_t>(sr::kDataAlign, round_up(num_dps, sr::kDataAlign));
   const size_t rows = static_cast<size_t>(num_vars) + 1;
   SR_TRY_CUDA(ctx, ctx->X.ensure(rows * static_cast<size_t>(ldx)));
   SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->X.p, 0, rows * ldx * sizeof(float), ctx->stream));
@@ -521,7 +515,7 @@ static sr_status set_data_host(sr_context *ctx, const float *X, const float *con
                                                " exceeds " + std::to_string(SR_MAX_VARS));
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  const int64_t ldx = std::max<int64_t>(1024, round_up(num_dps, 1024));
+  const int64_t ldx = std::max<int64_t>(sr::kDataAlign, round_up(num_dps, sr::kDataAlign));
   const size_t rows = static_cast<size_t>(num_vars) + 1;
   SR_TRY_CUDA(ctx, ctx->X.ensure(rows * static_cast<size_t>(ldx)));
   SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->X.p, 0, rows * ldx * sizeof(float), ctx->stream));
@@ -1091,3 +1085,33 @@ sr_status sr_validate_population(const sr_population *pop, int32_t num_vars, int
 }
 
 }  // extern "C"
+
+extern "C" sr_status sr_compile_population(const sr_population *pop, int32_t num_vars,
+                                           uint32_t *code, int64_t code_capacity,
+                                           int64_t *instr_offsets, int32_t *spill_slots) {
+  if (!pop || pop->num_exprs < 0 || num_vars < 0 || !instr_offsets || code_capacity < 0)
+    return SR_ERR_INVALID_ARGUMENT;
+  instr_offsets[0] = 0;
+  if (pop->num_exprs == 0) return SR_OK;
+  if (!pop->tokens || !pop->values || !pop->offsets || pop->offsets[0] != 0)
+    return SR_ERR_INVALID_ARGUMENT;
+  std::vector<sr::Instr> out;
+  for (int x = 0; x < pop->num_exprs; ++x) {
+    const int64_t o = pop->offsets[x];
+    const int64_t len = pop->offsets[x + 1] - o;
+    if (len <= 0) return SR_ERR_MALFORMED_EXPRESSION;
+    if (len > SR_MAX_TOKENS) return SR_ERR_EXPRESSION_TOO_LONG;
+    sr::ExprInfo info;
+    const sr_status s = sr::compile_expression(pop->tokens + o, pop->values + o,
+                                               static_cast<int>(len), num_vars, nullptr, out,
+                                               info, nullptr);
+    if (s != SR_OK) return s;
+    instr_offsets[x + 1] = static_cast<int64_t>(out.size());
+    if (spill_slots) spill_slots[x] = info.need;
+  }
+  if (code) {
+    if (static_cast<int64_t>(out.size()) > code_capacity) return SR_ERR_INVALID_ARGUMENT;
+    std::memcpy(code, out.data(), out.size() * sizeof(sr::Instr));
+  }
+  return SR_OK;
+}

@@ -76,12 +76,12 @@ struct PinnedBuf {
 // Launch shape of one interpreter launch.
 struct Plan {
   int dpt = 8;
-  int W = 8;
-  int smax = 0;
+  int W = 8;           // evaluating warps per block
+  int smax = 0;        // spill slots per warp
+  int G = 0;           // expressions per group
   int n_groups = 0;
+  int span = 0;        // datapoints per span
   int n_spans = 0;
-  int tiles_per_span = 0;
-  int n_tiles = 0;
   int blocks = 0;
   size_t smem = 0;
   int64_t items() const { return static_cast<int64_t>(n_groups) * n_spans; }

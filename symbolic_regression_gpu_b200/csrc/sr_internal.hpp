@@ -8,20 +8,31 @@
 // stack S whose slot for every access is fixed at compile time, so the device
 // never tracks a stack pointer.  Leaves are never instructions of their own:
 // every variable / constant / cached-subtree leaf is an operand of its parent
-// operator.  One instruction = one operator node of the tree (or a single MOV
-// when the whole expression is a leaf).
+// operator.  One instruction = one operator node of the tree (or a single
+// load when the whole expression is a leaf).  Every instruction has the
+// canonical form
 //
-//   Instr.w  bits 0..5   operator: reference token code 1..27, 32 = exp clamped
-//                        at 80 (extension), 0 = MOV (T = operand A)
-//            bits 6..8   kind of operand A (first popped, the left operand)
-//            bits 9..11  kind of operand B (right operand; kNone for unary)
-//            bit  12     spill: store T into S[spill slot] before executing
+//     [spill T -> S[slot]]  [T = leaf]  [b = operand]  T = op(T, b)
+//
+// so the device decodes no left/right operand roles: when the accumulator is
+// the right operand of a non-commutative operator the host emits the
+// reversed opcode, T = f(b, T).
+//
+//   Instr.w  bits 0..5   device opcode: reference token 1..27 (binary 1..9
+//                        as T = f(T, b), unary 10..27 as T = f(T)), 32 = exp
+//                        clamped at 80 (extension), 40 + k = reversed binary
+//                        k (T = f_k(b, T)) for non-commutative k, 0 = none
+//            bit  6      load: T = leaf A before the operator
+//            bits 7..8   kind of leaf A: 0 = variable row (shared memory),
+//                        1 = constant, 2 = cached subtree (global memory)
+//            bits 9..11  kind of operand b: 0 = none, 1 = spill slot,
+//                        2 = variable row, 3 = constant, 4 = cached subtree
+//            bit  12     spill: store T into S[spill slot] first
 //            bits 13..17 spill slot
-//   Instr.a  payload of operand A, Instr.b payload of operand B:
-//            kT: unused; kS: stack slot; kX: variable row; kC: float bits of
-//            the constant; kR: subtree-cache slot
-//   Instr.c  bits 0..9 / 10..19: constant index (token order) of operand A / B
-//            when that operand is a constant, 0x3FF otherwise (adjoint).
+//   Instr.a  payload of leaf A, Instr.b payload of operand b: spill slot /
+//            variable row / float bits of the constant / cache slot
+//   Instr.c  bits 0..9 / 10..19: constant index (token order) of leaf A /
+//            operand b when it is a constant, 0x3FF otherwise (adjoint).
 #pragma once
 #include <cstdint>
 #include <vector_types.h>
@@ -34,34 +45,34 @@
 
 namespace sr {
 
-enum : uint32_t {
-  kT = 0,     // accumulator
-  kS = 1,     // spilled stack slot (per-warp shared memory)
-  kX = 2,     // input variable row of the staged X tile (shared memory)
-  kC = 3,     // immediate constant
-  kR = 4,     // cached subtree value (global memory [slot][dp])
-  kNone = 7,  // no operand (unary)
-};
+// Kinds of leaf A (loaded into the accumulator).
+enum : uint32_t { kLeafX = 0, kLeafC = 1, kLeafR = 2 };
+// Kinds of operand b.
+enum : uint32_t { kBNone = 0, kBS = 1, kBX = 2, kBC = 3, kBR = 4 };
 
-constexpr uint32_t kOpMov = 0;
+constexpr uint32_t kOpNone = 0;
 constexpr uint32_t kOpExpClamp = 32;
+constexpr uint32_t kOpReversed = 40;  // 40 + k: T = f_k(b, T)
+constexpr uint32_t kLoadBit = 1u << 6;
 constexpr uint32_t kSpillBit = 1u << 12;
 constexpr uint32_t kNoConst = 0x3FFu;
 constexpr int kMaxSpillSlots = 16;  // S slots per warp supported by the kernels
-constexpr int kStages = 4;          // X tile ring depth
+constexpr int kBufs = 2;            // X span buffers per block
 
 struct alignas(16) Instr {
   uint32_t w, a, b, c;
 };
 
 SR_HD uint32_t instr_op(uint32_t w) { return w & 63u; }
-SR_HD uint32_t instr_ka(uint32_t w) { return (w >> 6) & 7u; }
-SR_HD uint32_t instr_kb(uint32_t w) { return (w >> 9) & 7u; }
+SR_HD bool instr_load(uint32_t w) { return (w & kLoadBit) != 0; }
+SR_HD uint32_t instr_leaf_kind(uint32_t w) { return (w >> 7) & 3u; }
+SR_HD uint32_t instr_b_kind(uint32_t w) { return (w >> 9) & 7u; }
 SR_HD bool instr_spill(uint32_t w) { return (w & kSpillBit) != 0; }
 SR_HD uint32_t instr_spill_slot(uint32_t w) { return (w >> 13) & 31u; }
-SR_HD uint32_t make_w(uint32_t op, uint32_t ka, uint32_t kb) {
-  return (op & 63u) | ((ka & 7u) << 6) | ((kb & 7u) << 9);
-}
+// Non-commutative binary operators get a reversed opcode.  ADD and MUL are
+// exactly commutative in IEEE arithmetic; MIN/MAX are treated as
+// non-commutative so that signed zeros keep the reference's operand order.
+SR_HD bool is_commutative_token(int tok) { return tok == 1 || tok == 3; }
 SR_HD bool is_binary_token(int tok) { return tok >= 1 && tok <= 9; }
 SR_HD bool is_unary_token(int tok) {
   return (tok >= 10 && tok <= 27) || tok == static_cast<int>(kOpExpClamp);
@@ -75,24 +86,27 @@ enum : int32_t {
 
 // Argument block of the interpreter kernel (passed by value).
 //
-// Work decomposition: expressions are sorted by modelled cost and cut into
-// groups of W (one expression per evaluating warp); the datapoint axis is cut
-// into tiles of 32*DPT datapoints and the tiles into spans.  A work item is
-// (span, group); items are numbered span-major and handed out by an atomic
-// counter to persistent blocks.  Each block streams the tiles of its item
-// through a kStages-deep ring of X tiles filled by the bulk-copy engine.
+// Work decomposition: expressions are sorted by modelled cost (descending)
+// and cut into groups of G; the datapoint axis is cut into spans of `span`
+// datapoints.  A work item is (span, group); items are numbered span-major
+// and handed out by an atomic counter to persistent blocks.  A block's
+// producer thread copies the item's X span (all V+1 rows) into one of two
+// shared-memory buffers with the bulk-copy engine; the block's evaluating
+// warps claim the group's expressions one at a time from a shared counter and
+// run each over the whole span, tile by tile (32*DPT datapoints per tile).
+// Warps never wait for each other inside an item.
 struct EvalArgs {
   const float *X;        // [(V+1)][ldx], y in row V
-  int64_t ldx;           // row stride (floats), multiple of 256
+  int64_t ldx;           // row stride (floats), multiple of 4096
   int64_t N;             // datapoints
   const Instr *code;     // all programs back to back
   const int64_t *code_off;   // [E] first instruction of each expression
   const int32_t *code_len;   // [E] instruction count
-  const int32_t *group_expr; // [n_groups * W] expression index or -1
+  const int32_t *group_expr; // [n_groups * G] expression index or -1 (tail)
   double2 *partial;      // [n_spans][E] (sum of squared errors, valid count)
   int32_t *work_counter; // zeroed before each launch
   int32_t *error;        // device error word
-  const float *cache;    // subtree cache [slot][ldc] (kR operands)
+  const float *cache;    // subtree cache [slot][ldc] (cached-subtree operands)
   int64_t ldc;
   float *pred;           // prediction output [row][ldp] (prediction mode)
   int64_t ldp;
@@ -101,10 +115,10 @@ struct EvalArgs {
   int32_t E;
   int32_t W;             // evaluating warps per block (block = (W+1) warps)
   int32_t smax;          // S slots per warp
+  int32_t G;             // expressions per group
   int32_t n_groups;
+  int32_t span;          // datapoints per span, multiple of 32*DPT
   int32_t n_spans;
-  int32_t tiles_per_span;
-  int32_t n_tiles;
 };
 
 }  // namespace sr

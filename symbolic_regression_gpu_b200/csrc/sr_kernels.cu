@@ -1,19 +1,20 @@
 // sr_kernels.cu — sm_100a kernels of the population evaluator.
 //
-//  interp_kernel<DPT, PRED>   persistent interpreter.  One producer warp per
-//                             block claims work items (span, group) from a
-//                             global counter and streams the span's X tiles
-//                             through a kStages-deep shared-memory ring with
-//                             the bulk-copy (TMA) engine, one
-//                             cp.async.bulk per X row, completion tracked by
-//                             mbarrier transaction counts.  Each of the W
-//                             evaluating warps runs one expression of the group
-//                             over every tile: 32 lanes x DPT datapoints per
-//                             instruction fetch, accumulator in registers,
-//                             spilled values in a per-warp shared stack.  The
-//                             epilogue either accumulates the squared error
-//                             (FP32 Kahan over a lane's DPT values, FP64 across
-//                             tiles and lanes) or stores the predictions.
+//  interp_kernel<DPT, PRED>   persistent interpreter.  One producer thread
+//                             per block claims work items (span, group) from
+//                             a global counter and copies the item's X span
+//                             (every row) into one of two shared-memory
+//                             buffers with the bulk-copy (TMA) engine, one
+//                             cp.async.bulk per row, completion tracked by
+//                             mbarrier transaction counts.  The W evaluating
+//                             warps claim the group's expressions from a
+//                             shared counter and run each over the whole span:
+//                             32 lanes x DPT datapoints per instruction fetch,
+//                             accumulator in registers, spilled values in a
+//                             per-warp shared stack.  The epilogue either
+//                             accumulates the squared error (FP32 Kahan over a
+//                             lane's DPT values, FP64 across tiles and lanes)
+//                             or stores the predictions.
 //  finalize_kernel            per-expression combination of span partials in
 //                             a fixed order: mse = sum / count.
 //  plain_kernel               baseline with the reference's launch shape
@@ -39,11 +40,11 @@ namespace {
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s per mbarrier wait
 constexpr uint64_t kDrainLimitNs = 100000000ull;  // 100 ms on error paths
 
-struct alignas(16) StageDesc {
+struct alignas(16) ItemDesc {
   int32_t item;   // work item, -1 = no more work
-  int32_t tile;   // tile index along the datapoint axis
-  int32_t last;   // last tile of the item's span
-  int32_t pad;
+  int32_t group;
+  int32_t span;
+  int32_t claim;  // next expression of the group to hand out
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -180,101 +181,245 @@ __device__ __forceinline__ void stg_vec(float *base, int lane,
         make_float4(v[4 * h + 0], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
 }
 
-// Operand fetch; `kind` and `payload` are warp-uniform.
+// ---- out-of-line 4-wide operator routines ---------------------------------
+// Every routine that expands to more than a handful of instructions (CUDA's
+// accurate transcendentals, IEEE division / reciprocal / square root, powf)
+// exists once, four datapoints wide, instead of being inlined DPT times into
+// each opcode of the dispatch switch: that keeps the interpreter's code small
+// enough for the instruction cache.
+#ifndef SR_INLINE_MATH
+#define SR_INLINE_MATH 0
+#endif
+#if SR_INLINE_MATH
+#define SR_OUTLINE __forceinline__
+#else
+#define SR_OUTLINE __noinline__
+#endif
+#define SR_V1(NAME, EXPR)                                                   \
+  __device__ SR_OUTLINE float4 NAME(float4 v) {                             \
+    float4 r;                                                               \
+    { const float x = v.x; r.x = (EXPR); }                                  \
+    { const float x = v.y; r.y = (EXPR); }                                  \
+    { const float x = v.z; r.z = (EXPR); }                                  \
+    { const float x = v.w; r.w = (EXPR); }                                  \
+    return r;                                                               \
+  }
+#define SR_V2(NAME, EXPR)                                                   \
+  __device__ SR_OUTLINE float4 NAME(float4 u, float4 v) {                   \
+    float4 r;                                                               \
+    { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
+    { const float x = u.y, y = v.y; r.y = (EXPR); }                         \
+    { const float x = u.z, y = v.z; r.z = (EXPR); }                         \
+    { const float x = u.w, y = v.w; r.w = (EXPR); }                         \
+    return r;                                                               \
+  }
+SR_V1(v_sin, sinf(x))
+SR_V1(v_cos, cosf(x))
+SR_V1(v_tan, tanf(x))
+SR_V1(v_sinh, sinhf(x))
+SR_V1(v_cosh, coshf(x))
+SR_V1(v_tanh, tanhf(x))
+SR_V1(v_exp, expf(x))
+SR_V1(v_log, logf(x))
+SR_V1(v_asin, asinf(x))
+SR_V1(v_acos, acosf(x))
+SR_V1(v_atan, atanf(x))
+SR_V1(v_rcp, __frcp_rn(x))
+SR_V1(v_sqrt, __fsqrt_rn(x))
+SR_V2(v_div, __fdiv_rn(x, y))
+SR_V2(v_pow, powf(x, y))
+#undef SR_V1
+#undef SR_V2
+
 template <int DPT>
-__device__ __forceinline__ void fetch(uint32_t kind, uint32_t payload,
-                                      float (&v)[DPT], const float (&T)[DPT],
-                                      const float *xs, const float *ss,
-                                      int lane, const float *cache, int64_t ldc,
-                                      int64_t dp0) {
+__device__ __forceinline__ float4 quad(const float (&v)[DPT], int h) {
+  return make_float4(v[4 * h + 0], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+}
+template <int DPT>
+__device__ __forceinline__ void unquad(float (&v)[DPT], int h, float4 q) {
+  v[4 * h + 0] = q.x;
+  v[4 * h + 1] = q.y;
+  v[4 * h + 2] = q.z;
+  v[4 * h + 3] = q.w;
+}
+
+// T = leaf; kind and payload are warp-uniform.
+template <int DPT>
+__device__ __forceinline__ void load_leaf(uint32_t kind, uint32_t payload, float (&T)[DPT],
+                                          const float *xs, int xrs, int lane,
+                                          const float *cache, int64_t ldc, int64_t dp0) {
+  if (kind == kLeafX) {
+    lds_vec<DPT>(xs + payload * xrs, lane, T);
+  } else if (kind == kLeafC) {
+    const float c = __uint_as_float(payload);
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) T[k] = c;
+  } else {
+    ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, T);
+  }
+}
+
+// b = operand; kind and payload are warp-uniform, kind != kBNone.
+template <int DPT>
+__device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, float (&b)[DPT],
+                                             const float *xs, int xrs, const float *ss,
+                                             int lane, const float *cache, int64_t ldc,
+                                             int64_t dp0) {
   constexpr int TILE = 32 * DPT;
-  switch (kind) {
-    case kT:
+  if (kind == kBC) {
+    const float c = __uint_as_float(payload);
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) v[k] = T[k];
-      break;
-    case kS:
-      lds_vec<DPT>(ss + payload * TILE, lane, v);
-      break;
-    case kX:
-      lds_vec<DPT>(xs + payload * TILE, lane, v);
-      break;
-    case kR:
-      ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, v);
-      break;
-    default: {  // kC
-      const float c = __uint_as_float(payload);
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) v[k] = c;
-    } break;
+    for (int k = 0; k < DPT; ++k) b[k] = c;
+  } else if (kind == kBR) {
+    ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, b);
+  } else if (kind == kBX) {
+    lds_vec<DPT>(xs + payload * xrs, lane, b);
+  } else {
+    lds_vec<DPT>(ss + payload * TILE, lane, b);
   }
 }
 
-#define SR_UNARY(OPC, EXPR)                 \
-  case OPC: {                               \
-    _Pragma("unroll") for (int k = 0; k < DPT; ++k) { \
-      const float x = a[k];                 \
-      T[k] = (EXPR);                        \
-    }                                       \
-  } break;
-#define SR_BINARY(OPC, EXPR)                \
-  case OPC: {                               \
-    _Pragma("unroll") for (int k = 0; k < DPT; ++k) { \
-      const float x = a[k];                 \
-      const float y = b[k];                 \
-      T[k] = (EXPR);                        \
-    }                                       \
-  } break;
+#define SR_EACH(STMT)                                            \
+  {                                                              \
+    _Pragma("unroll") for (int k = 0; k < DPT; ++k) { STMT; }   \
+  }                                                              \
+  break;
+#define SR_CALL1(FN)                                                      \
+  {                                                                       \
+    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h)                   \
+        unquad<DPT>(T, h, FN(quad<DPT>(T, h)));                           \
+  }                                                                       \
+  break;
+#define SR_CALL2(FN, X, Y)                                                \
+  {                                                                       \
+    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h)                   \
+        unquad<DPT>(T, h, FN(quad<DPT>(X, h), quad<DPT>(Y, h)));          \
+  }                                                                       \
+  break;
 
-// T = op(a, b) for DPT datapoints; the switch is on a warp-uniform opcode.
+// T = op(T, b) (T = op(T) for unary operators) for DPT datapoints; the
+// switch is on a warp-uniform opcode.  Semantics: sr_ops.cuh.
 template <int DPT>
-__device__ __forceinline__ void apply_op(uint32_t op, const float (&a)[DPT],
-                                         const float (&b)[DPT], float (&T)[DPT]) {
+__device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b)[DPT]) {
+  const float kNaN = qnan();
   switch (op) {
-    SR_UNARY(0, x)
-    SR_BINARY(1, __fadd_rn(x, y))
-    SR_BINARY(2, __fsub_rn(x, y))
-    SR_BINARY(3, __fmul_rn(x, y))
-    SR_BINARY(4, (y == 0.0f) ? qnan() : __fdiv_rn(x, y))
-    SR_BINARY(5, powf(x, y))
-    SR_BINARY(6, fminf(x, y))
-    SR_BINARY(7, fmaxf(x, y))
-    SR_BINARY(8, __fdiv_rn(x, loose_denom(y)))
-    SR_BINARY(9, (x == 0.0f && y == 0.0f) ? 0.0f : powf(fabsf(x), y))
-    SR_UNARY(10, sinf(x))
-    SR_UNARY(11, cosf(x))
-    SR_UNARY(12, tanf(x))
-    SR_UNARY(13, sinhf(x))
-    SR_UNARY(14, coshf(x))
-    SR_UNARY(15, tanhf(x))
-    SR_UNARY(16, expf(x))
-    SR_UNARY(17, logf(x))
-    SR_UNARY(18, __frcp_rn(x))
-    SR_UNARY(19, asinf(x))
-    SR_UNARY(20, acosf(x))
-    SR_UNARY(21, atanf(x))
-    SR_UNARY(22, (x == 0.0f) ? -1e9f : logf(fabsf(x)))
-    SR_UNARY(23, __frcp_rn(loose_denom(x)))
-    SR_UNARY(24, fabsf(x))
-    SR_UNARY(25, -x)
-    SR_UNARY(26, __fsqrt_rn(x))
-    SR_UNARY(27, __fsqrt_rn(fabsf(x)))
-    SR_UNARY(32, expf(fminf(x, 80.0f)))
-    default: {
+    case 0: break;
+    case 1: SR_EACH(T[k] = __fadd_rn(T[k], b[k]))
+    case 2: SR_EACH(T[k] = __fsub_rn(T[k], b[k]))
+    case 42: SR_EACH(T[k] = __fsub_rn(b[k], T[k]))
+    case 3: SR_EACH(T[k] = __fmul_rn(T[k], b[k]))
+    case 4: {  // DIV: NaN when the divisor is 0
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = 0.0f;
+      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_div(quad<DPT>(T, h), quad<DPT>(b, h)));
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = (b[k] == 0.0f) ? kNaN : T[k];
     } break;
+    case 44: {  // reversed DIV: b / T
+      float den[DPT];
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) den[k] = T[k];
+#pragma unroll
+      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_div(quad<DPT>(b, h), quad<DPT>(den, h)));
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = (den[k] == 0.0f) ? kNaN : T[k];
+    } break;
+    case 5: SR_CALL2(v_pow, T, b)
+    case 45: SR_CALL2(v_pow, b, T)
+    case 6: SR_EACH(T[k] = fminf(T[k], b[k]))
+    case 46: SR_EACH(T[k] = fminf(b[k], T[k]))
+    case 7: SR_EACH(T[k] = fmaxf(T[k], b[k]))
+    case 47: SR_EACH(T[k] = fmaxf(b[k], T[k]))
+    case 8: {  // LOOSE_DIV: T / protected(b)
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) b[k] = loose_denom(b[k]);
+    }
+      SR_CALL2(v_div, T, b)
+    case 48: {  // reversed LOOSE_DIV: b / protected(T)
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = loose_denom(T[k]);
+    }
+      SR_CALL2(v_div, b, T)
+    case 9: {  // LOOSE_POW: 0^0 = 0, else |T|^b
+      bool z[DPT];
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) {
+        z[k] = (T[k] == 0.0f && b[k] == 0.0f);
+        T[k] = fabsf(T[k]);
+      }
+#pragma unroll
+      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_pow(quad<DPT>(T, h), quad<DPT>(b, h)));
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = z[k] ? 0.0f : T[k];
+    } break;
+    case 49: {  // reversed LOOSE_POW: 0^0 = 0, else |b|^T
+      bool z[DPT];
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) {
+        z[k] = (T[k] == 0.0f && b[k] == 0.0f);
+        b[k] = fabsf(b[k]);
+      }
+#pragma unroll
+      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_pow(quad<DPT>(b, h), quad<DPT>(T, h)));
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = z[k] ? 0.0f : T[k];
+    } break;
+    case 10: SR_CALL1(v_sin)
+    case 11: SR_CALL1(v_cos)
+    case 12: SR_CALL1(v_tan)
+    case 13: SR_CALL1(v_sinh)
+    case 14: SR_CALL1(v_cosh)
+    case 15: SR_CALL1(v_tanh)
+    case 16: SR_CALL1(v_exp)
+    case 17: SR_CALL1(v_log)
+    case 18: SR_CALL1(v_rcp)
+    case 19: SR_CALL1(v_asin)
+    case 20: SR_CALL1(v_acos)
+    case 21: SR_CALL1(v_atan)
+    case 22: {  // LOOSE_LOG: -1e9 at 0, else log|T|
+      bool z[DPT];
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) {
+        z[k] = (T[k] == 0.0f);
+        T[k] = fabsf(T[k]);
+      }
+#pragma unroll
+      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_log(quad<DPT>(T, h)));
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = z[k] ? -1e9f : T[k];
+    } break;
+    case 23: {  // LOOSE_INV: 1 / protected(T)
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = loose_denom(T[k]);
+    }
+      SR_CALL1(v_rcp)
+    case 24: SR_EACH(T[k] = fabsf(T[k]))
+    case 25: SR_EACH(T[k] = -T[k])
+    case 26: SR_CALL1(v_sqrt)
+    case 27: {
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = fabsf(T[k]);
+    }
+      SR_CALL1(v_sqrt)
+    case 32: {  // exp clamped at 80 (extension)
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) T[k] = fminf(T[k], 80.0f);
+    }
+      SR_CALL1(v_exp)
+    default: SR_EACH(T[k] = 0.0f)
   }
 }
 
-#undef SR_UNARY
-#undef SR_BINARY
+#undef SR_EACH
+#undef SR_CALL1
+#undef SR_CALL2
 
 // Run one compiled program over the warp's DPT x 32 datapoints of a tile.
+// xs points at the tile's first datapoint of X row 0; rows are xrs floats
+// apart.
 template <int DPT>
 __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
-                                            int len, const float *xs, float *ss,
-                                            int lane, const float *cache,
+                                            int len, const float *xs, int xrs,
+                                            float *ss, int lane, const float *cache,
                                             int64_t ldc, int64_t dp0,
                                             float (&T)[DPT]) {
   constexpr int TILE = 32 * DPT;
@@ -287,50 +432,34 @@ __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
     const uint4 nxt = ldg_instr(code + i + 1);
     const uint32_t w = ins.x;
     if (instr_spill(w)) sts_vec<DPT>(ss + instr_spill_slot(w) * TILE, lane, T);
-    float a[DPT], b[DPT];
-    fetch<DPT>(instr_ka(w), ins.y, a, T, xs, ss, lane, cache, ldc, dp0);
-    const uint32_t kb = instr_kb(w);
-    if (kb != kNone) {
-      fetch<DPT>(kb, ins.z, b, T, xs, ss, lane, cache, ldc, dp0);
-    } else {
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) b[k] = 0.0f;
-    }
-    apply_op<DPT>(instr_op(w), a, b, T);
+    if (instr_load(w))
+      load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
+    float b[DPT];
+    const uint32_t bk = instr_b_kind(w);
+    if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, xrs, ss, lane, cache, ldc, dp0);
+    apply_op<DPT>(instr_op(w), T, b);
     ins = nxt;
   }
 }
 
 template <int DPT, bool PRED>
-struct LaunchBounds;
-template <bool PRED>
-struct LaunchBounds<8, PRED> {
-  static constexpr int kMinBlocks = 2;
-};
-template <bool PRED>
-struct LaunchBounds<4, PRED> {
-  static constexpr int kMinBlocks = 3;
-};
-
-template <int DPT, bool PRED>
-__global__ void __launch_bounds__(kMaxBlockThreads,
-                                  (LaunchBounds<DPT, PRED>::kMinBlocks))
-    interp_kernel(const EvalArgs p) {
+__global__ void __launch_bounds__(kMaxBlockThreads, 1) interp_kernel(const EvalArgs p) {
   constexpr int TILE = 32 * DPT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int W = p.W;
   const int rows = p.V + 1;
-  float *ring = reinterpret_cast<float *>(smem_raw);
-  float *sreg = ring + static_cast<size_t>(kStages) * rows * TILE;
-  StageDesc *desc =
-      reinterpret_cast<StageDesc *>(sreg + static_cast<size_t>(W) * p.smax * TILE);
-  uint64_t *full = reinterpret_cast<uint64_t *>(desc + kStages);
-  uint64_t *empty = full + kStages;
+  const int span = p.span;
+  float *xbuf = reinterpret_cast<float *>(smem_raw);
+  float *sreg = xbuf + static_cast<size_t>(kBufs) * rows * span;
+  ItemDesc *desc =
+      reinterpret_cast<ItemDesc *>(sreg + static_cast<size_t>(W) * p.smax * TILE);
+  uint64_t *full = reinterpret_cast<uint64_t *>(desc + kBufs);
+  uint64_t *empty = full + kBufs;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kBufs; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], static_cast<uint32_t>(W));
     }
@@ -343,125 +472,118 @@ __global__ void __launch_bounds__(kMaxBlockThreads,
   if (warp == W) {
     // ---------------- producer: one thread ----------------
     if (lane != 0) return;
-    uint32_t stage = 0, phase = 0;
-    uint32_t armed = 0;                 // stages with a copy in flight
-    uint32_t armed_parity[kStages] = {};
-    const uint32_t tile_bytes = static_cast<uint32_t>(TILE * sizeof(float));
+    uint32_t buf = 0, phase = 0;
+    uint32_t armed = 0;  // buffers with a copy in flight
+    uint32_t armed_parity0 = 0, armed_parity1 = 0;
+    const uint32_t row_bytes = static_cast<uint32_t>(span) * sizeof(float);
     for (;;) {
       const int item = atomicAdd(p.work_counter, 1);
-      if (item >= n_items) {
-        if (mbar_wait(&empty[stage], phase ^ 1u, p.error)) {
-          desc[stage] = StageDesc{-1, 0, 0, 0};
-          mbar_arrive(&full[stage]);
-        }
+      if (!mbar_wait(&empty[buf], phase ^ 1u, p.error)) {
+        // Let copies already issued land before the block exits.
+        if (armed & 1u) mbar_drain(&full[0], armed_parity0);
+        if (armed & 2u) mbar_drain(&full[1], armed_parity1);
         return;
       }
-      const int span = item / p.n_groups;
-      const int t0 = span * p.tiles_per_span;
-      const int t1 = min(p.n_tiles, t0 + p.tiles_per_span);
-      for (int t = t0; t < t1; ++t) {
-        if (!mbar_wait(&empty[stage], phase ^ 1u, p.error)) {
-          // Let copies already issued land before the block exits.
-          for (int s = 0; s < kStages; ++s)
-            if (armed & (1u << s)) mbar_drain(&full[s], armed_parity[s]);
-          return;
-        }
-        // The consumers released this stage, so its previous copy landed.
-        armed &= ~(1u << stage);
-        desc[stage] = StageDesc{item, t, t == t1 - 1 ? 1 : 0, 0};
-        mbar_arrive_expect_tx(&full[stage], tile_bytes * rows);
-        const float *src = p.X + static_cast<int64_t>(t) * TILE;
-        float *dst = ring + static_cast<size_t>(stage) * rows * TILE;
-        for (int v = 0; v < rows; ++v)
-          bulk_g2s(dst + v * TILE, src + v * p.ldx, tile_bytes, &full[stage]);
-        armed |= 1u << stage;
-        armed_parity[stage] = phase;
-        if (++stage == kStages) {
-          stage = 0;
-          phase ^= 1u;
-        }
+      // The consumers released this buffer, so its previous copy landed.
+      armed &= ~(1u << buf);
+      if (item >= n_items) {
+        desc[buf] = ItemDesc{-1, 0, 0, 0};
+        mbar_arrive(&full[buf]);
+        return;
+      }
+      const int group = item % p.n_groups;
+      const int sp = item / p.n_groups;
+      desc[buf] = ItemDesc{item, group, sp, 0};
+      mbar_arrive_expect_tx(&full[buf], row_bytes * rows);
+      const float *src = p.X + static_cast<int64_t>(sp) * span;
+      float *dst = xbuf + static_cast<size_t>(buf) * rows * span;
+      for (int v = 0; v < rows; ++v)
+        bulk_g2s(dst + static_cast<size_t>(v) * span, src + v * p.ldx, row_bytes, &full[buf]);
+      armed |= 1u << buf;
+      if (buf == 0) armed_parity0 = phase;
+      else armed_parity1 = phase;
+      if (++buf == kBufs) {
+        buf = 0;
+        phase ^= 1u;
       }
     }
   }
 
   // ---------------- evaluating warps ----------------
   float *ss = sreg + static_cast<size_t>(warp) * p.smax * TILE;
-  uint32_t stage = 0, phase = 0;
-  int cur_item = -1, e = -1, span = 0, len = 0;
-  int64_t off = 0;
-  double acc = 0.0;
-  int cnt = 0;
+  const int tiles = span / TILE;
+  uint32_t buf = 0, phase = 0;
   for (;;) {
-    if (!mbar_wait(&full[stage], phase, p.error)) return;
-    const StageDesc d = desc[stage];
+    if (!mbar_wait(&full[buf], phase, p.error)) return;
+    const ItemDesc d = desc[buf];
     if (d.item < 0) return;
-    if (d.item != cur_item) {
-      cur_item = d.item;
-      const int group = cur_item % p.n_groups;
-      span = cur_item / p.n_groups;
-      e = p.group_expr[group * W + warp];
-      if (e >= 0) {
-        off = p.code_off[e];
-        len = p.code_len[e];
-      }
-      acc = 0.0;
-      cnt = 0;
-    }
-    if (e >= 0) {
-      const float *xs = ring + static_cast<size_t>(stage) * rows * TILE;
-      const int64_t dp0 = static_cast<int64_t>(d.tile) * TILE;
-      float T[DPT];
-      run_program<DPT>(p.code + off, len, xs, ss, lane, p.cache, p.ldc, dp0, T);
-      if constexpr (PRED) {
-        stg_vec<DPT>(p.pred + static_cast<int64_t>(p.pred_row[e]) * p.ldp + dp0,
-                     lane, T);
-      } else {
-        float y[DPT];
-        lds_vec<DPT>(xs + p.V * TILE, lane, y);
-        float sq[DPT];
-        float s = 0.0f, c = 0.0f;  // Kahan over the lane's DPT values
-        int nv = 0;
+    const float *xb = xbuf + static_cast<size_t>(buf) * rows * span;
+    const int64_t dp_span = static_cast<int64_t>(d.span) * span;
+    for (;;) {
+      int j = 0;
+      if (lane == 0) j = atomicAdd(&desc[buf].claim, 1);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      if (j >= p.G) break;
+      const int e = p.group_expr[static_cast<int64_t>(d.group) * p.G + j];
+      if (e < 0) break;  // groups are padded at their end only
+      const Instr *code = p.code + p.code_off[e];
+      const int len = p.code_len[e];
+      double acc = 0.0;
+      int cnt = 0;
+      for (int t = 0; t < tiles; ++t) {
+        const int64_t dp0 = dp_span + static_cast<int64_t>(t) * TILE;
+        if (dp0 >= p.N) break;  // tail of the last span
+        const float *xs = xb + t * TILE;
+        float T[DPT];
+        run_program<DPT>(code, len, xs, span, ss, lane, p.cache, p.ldc, dp0, T);
+        if constexpr (PRED) {
+          stg_vec<DPT>(p.pred + static_cast<int64_t>(p.pred_row[e]) * p.ldp + dp0, lane, T);
+        } else {
+          float y[DPT];
+          lds_vec<DPT>(xs + p.V * span, lane, y);
+          float sq[DPT];
+          float s = 0.0f, c = 0.0f;  // Kahan over the lane's DPT values
+          int nv = 0;
 #pragma unroll
-        for (int k = 0; k < DPT; ++k) {
-          const int64_t dp = dp0 + (k / 4) * 128 + lane * 4 + (k % 4);
-          const bool valid = (dp < p.N) && isfinite(T[k]);
-          const float df = __fsub_rn(T[k], y[k]);
-          sq[k] = valid ? __fmul_rn(df, df) : 0.0f;
-          nv += valid ? 1 : 0;
-          const float yk = __fsub_rn(sq[k], c);
-          const float t = __fadd_rn(s, yk);
-          c = __fsub_rn(__fsub_rn(t, s), yk);
-          s = t;
-        }
-        double tile_sum = static_cast<double>(s) - static_cast<double>(c);
-        if (!isfinite(tile_sum)) {
-          // FP32 overflow of the running sum (or an infinite square): redo in
-          // FP64, which is exact for up to DPT finite squares and gives +Inf
-          // when one square is infinite, like the reference's double sum.
-          tile_sum = 0.0;
+          for (int k = 0; k < DPT; ++k) {
+            const int64_t dp = dp0 + (k / 4) * 128 + lane * 4 + (k % 4);
+            const bool valid = (dp < p.N) && isfinite(T[k]);
+            const float df = __fsub_rn(T[k], y[k]);
+            sq[k] = valid ? __fmul_rn(df, df) : 0.0f;
+            nv += valid ? 1 : 0;
+            const float yk = __fsub_rn(sq[k], c);
+            const float tt = __fadd_rn(s, yk);
+            c = __fsub_rn(__fsub_rn(tt, s), yk);
+            s = tt;
+          }
+          double tile_sum = static_cast<double>(s) - static_cast<double>(c);
+          if (!isfinite(tile_sum)) {
+            // FP32 overflow of the running sum (or an infinite square): redo
+            // in FP64, which is exact for DPT finite squares and gives +Inf
+            // when one square is infinite, like the reference's double sum.
+            tile_sum = 0.0;
 #pragma unroll
-          for (int k = 0; k < DPT; ++k) tile_sum += static_cast<double>(sq[k]);
+            for (int k = 0; k < DPT; ++k) tile_sum += static_cast<double>(sq[k]);
+          }
+          acc += tile_sum;
+          cnt += nv;
         }
-        acc += tile_sum;
-        cnt += nv;
       }
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[stage]);
-    if constexpr (!PRED) {
-      if (d.last && e >= 0) {
+      if constexpr (!PRED) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           acc += __shfl_xor_sync(0xffffffffu, acc, o);
           cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         }
         if (lane == 0)
-          p.partial[static_cast<int64_t>(span) * p.E + e] =
+          p.partial[static_cast<int64_t>(d.span) * p.E + e] =
               make_double2(acc, static_cast<double>(cnt));
       }
     }
-    if (++stage == kStages) {
-      stage = 0;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[buf]);
+    if (++buf == kBufs) {
+      buf = 0;
       phase ^= 1u;
     }
   }
@@ -592,11 +714,11 @@ __global__ void mufu_pipe_kernel(float *out, int iters) {
 
 }  // namespace
 
-size_t interp_smem_bytes(int dpt, int W, int V, int smax) {
+size_t interp_smem_bytes(int dpt, int W, int V, int smax, int span) {
   const size_t tile = 32u * static_cast<size_t>(dpt);
-  return (static_cast<size_t>(kStages) * (V + 1) * tile +
+  return (static_cast<size_t>(kBufs) * (V + 1) * span +
           static_cast<size_t>(W) * smax * tile) * sizeof(float) +
-         kStages * sizeof(StageDesc) + 2 * kStages * sizeof(uint64_t);
+         kBufs * sizeof(ItemDesc) + 2 * kBufs * sizeof(uint64_t);
 }
 
 template <int DPT, bool PRED>

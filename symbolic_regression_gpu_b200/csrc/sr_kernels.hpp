@@ -8,12 +8,13 @@
 
 namespace sr {
 
-constexpr int kMaxWarps = 8;                        // evaluating warps per block
+constexpr int kMaxWarps = 16;                       // evaluating warps per block
 constexpr int kMaxBlockThreads = (kMaxWarps + 1) * 32;  // + producer warp
+constexpr int64_t kDataAlign = 4096;               // X / cache row stride multiple
 constexpr int kPlainStack = 128;                    // plain kernel stack depth
 
 // Dynamic shared memory of interp_kernel for a launch shape.
-size_t interp_smem_bytes(int dpt, int W, int V, int smax);
+size_t interp_smem_bytes(int dpt, int W, int V, int smax, int span);
 // Sets the dynamic-smem attribute and returns resident blocks per SM.
 cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
                              int *blocks_per_sm);

@@ -102,8 +102,8 @@ namespace {
 struct Node {
   bool leaf = false;
   int32_t op = 0;          // operator token
-  uint32_t lk = kC;        // leaf operand kind
-  uint32_t lp = 0;         // leaf operand payload
+  uint32_t lk = kLeafC;    // leaf kind (kLeafX / kLeafC / kLeafR)
+  uint32_t lp = 0;         // leaf payload
   uint32_t lconst = kNoConst;
   int32_t left = -1;       // first popped operand (operators)
   int32_t right = -1;      // second popped operand (binary)
@@ -123,67 +123,86 @@ inline int var_index(double v) {
   return static_cast<int>(v);
 }
 
+inline uint32_t b_kind_of_leaf(uint32_t lk) {
+  return lk == kLeafX ? kBX : (lk == kLeafC ? kBC : kBR);
+}
+
+// Opcode computing T = f(b, T) for binary token f.
+inline uint32_t reversed(int tok) {
+  return is_commutative_token(tok) ? static_cast<uint32_t>(tok)
+                                   : kOpReversed + static_cast<uint32_t>(tok);
+}
+
 struct Emitter {
   const std::vector<Node> &nodes;
   std::vector<Instr> &out;
   int pending_spill = -1;
   int sp = 0;
 
-  void emit(uint32_t op, uint32_t ka, uint32_t pa, uint32_t ca, uint32_t kb,
-            uint32_t pb, uint32_t cb) {
+  // [spill] [T = load] [b = operand] T = op(T, b)
+  void emit(uint32_t op, const Node *load, uint32_t bk, uint32_t bp, uint32_t bc) {
     Instr ins;
-    ins.w = make_w(op, ka, kb);
+    ins.w = (op & 63u) | ((bk & 7u) << 9);
+    uint32_t ac = kNoConst;
+    ins.a = 0;
+    if (load) {
+      ins.w |= kLoadBit | ((load->lk & 3u) << 7);
+      ins.a = load->lp;
+      ac = load->lconst;
+    }
     if (pending_spill >= 0) {
       ins.w |= kSpillBit | (static_cast<uint32_t>(pending_spill) << 13);
       pending_spill = -1;
     }
-    ins.a = pa;
-    ins.b = pb;
-    ins.c = (ca & 0x3FFu) | ((cb & 0x3FFu) << 10);
+    ins.b = bp;
+    ins.c = (ac & 0x3FFu) | ((bc & 0x3FFu) << 10);
     out.push_back(ins);
+  }
+
+  void emit_b_leaf(uint32_t op, const Node *load, const Node &b) {
+    emit(op, load, b_kind_of_leaf(b.lk), b.lp, b.lconst);
   }
 
   void gen(int n) {
     const Node &nd = nodes[n];
     if (nd.leaf) {
-      emit(kOpMov, nd.lk, nd.lp, nd.lconst, kNone, 0, kNoConst);
+      emit(kOpNone, &nd, kBNone, 0, kNoConst);
       return;
     }
     const Node &L = nodes[nd.left];
+    const uint32_t op = static_cast<uint32_t>(nd.op);
     if (nd.right < 0) {  // unary
       if (L.leaf) {
-        emit(nd.op, L.lk, L.lp, L.lconst, kNone, 0, kNoConst);
+        emit(op, &L, kBNone, 0, kNoConst);
       } else {
         gen(nd.left);
-        emit(nd.op, kT, 0, kNoConst, kNone, 0, kNoConst);
+        emit(op, nullptr, kBNone, 0, kNoConst);
       }
       return;
     }
     const Node &R = nodes[nd.right];
     if (L.leaf && R.leaf) {
-      emit(nd.op, L.lk, L.lp, L.lconst, R.lk, R.lp, R.lconst);
+      emit_b_leaf(op, &L, R);              // T = L; T = f(T, R)
     } else if (R.leaf) {
       gen(nd.left);
-      emit(nd.op, kT, 0, kNoConst, R.lk, R.lp, R.lconst);
+      emit_b_leaf(op, nullptr, R);         // T = f(T=L, R)
     } else if (L.leaf) {
       gen(nd.right);
-      emit(nd.op, L.lk, L.lp, L.lconst, kT, 0, kNoConst);
+      emit_b_leaf(reversed(nd.op), nullptr, L);  // T = f(L, T=R)
     } else {
       // Both operands are operator subtrees: evaluate the one needing more
       // spill slots first (ties: the right one, the reference's own order),
       // park it in S[sp], evaluate the other into T, combine.
       const bool left_first = L.need > R.need;
-      const int first = left_first ? nd.left : nd.right;
-      const int second = left_first ? nd.right : nd.left;
-      gen(first);
+      gen(left_first ? nd.left : nd.right);
       const int slot = sp++;
       pending_spill = slot;
-      gen(second);
+      gen(left_first ? nd.right : nd.left);
       --sp;
       if (left_first)
-        emit(nd.op, kS, static_cast<uint32_t>(slot), kNoConst, kT, 0, kNoConst);
+        emit(reversed(nd.op), nullptr, kBS, static_cast<uint32_t>(slot), kNoConst);  // f(S, T)
       else
-        emit(nd.op, kT, 0, kNoConst, kS, static_cast<uint32_t>(slot), kNoConst);
+        emit(op, nullptr, kBS, static_cast<uint32_t>(slot), kNoConst);  // f(T, S)
     }
   }
 };
@@ -278,23 +297,23 @@ sr_status compile_expression(const int32_t *tok, const double *val, int len,
     if (e < 0) {
       const int k = -e - 1;
       nd.leaf = true;
-      nd.lk = kR;
+      nd.lk = kLeafR;
       nd.lp = static_cast<uint32_t>(hints[k]);
     } else {
       const int t = tok[e];
       if (t == SR_TOK_CONST) {
         nd.leaf = true;
-        nd.lk = kC;
+        nd.lk = kLeafC;
         nd.lp = float_bits(static_cast<float>(val[e]));
         nd.lconst = static_cast<uint32_t>(const_idx[e]);
       } else if (t == SR_TOK_VAR) {
         nd.leaf = true;
         const int v = var_index(val[e]);
         if (v >= 0 && v < num_vars) {
-          nd.lk = kX;
+          nd.lk = kLeafX;
           nd.lp = static_cast<uint32_t>(v);
         } else {
-          nd.lk = kC;  // reference CPU pushes 0.0f (cl_cpu_eval.cpp:73-75)
+          nd.lk = kLeafC;  // reference CPU pushes 0.0f (cl_cpu_eval.cpp:73-75)
           nd.lp = float_bits(0.0f);
         }
       } else {
@@ -357,14 +376,15 @@ sr_status compile_expression(const int32_t *tok, const double *val, int len,
   double sfu = 0, fp = 0;
   for (size_t i = first; i < out.size(); ++i) {
     const uint32_t w = out[i].w;
-    const int op = static_cast<int>(instr_op(w));
-    cost += 2.0f + op_cost(op);
-    const uint32_t ka = instr_ka(w), kb = instr_kb(w);
-    if (ka == kS || ka == kX || ka == kR) cost += 0.5f;
-    if (kb == kS || kb == kX || kb == kR) cost += 0.5f;
+    uint32_t op = instr_op(w);
+    if (op > kOpReversed) op -= kOpReversed;
+    cost += 2.0f + op_cost(static_cast<int>(op));
+    if (instr_load(w) && instr_leaf_kind(w) != kLeafC) cost += 0.5f;
+    const uint32_t bk = instr_b_kind(w);
+    if (bk == kBS || bk == kBX || bk == kBR) cost += 0.5f;
     if (instr_spill(w)) cost += 0.5f;
     double s, f;
-    declared_op_work(op, &s, &f);
+    declared_op_work(static_cast<int>(op), &s, &f);
     sfu += s;
     fp += f;
   }

@@ -281,3 +281,22 @@ def validate(pop: Population, num_vars: int):
     if st != _lib.SR_OK:
         raise _lib.SrError(st, f"expression {bad.value}: {_lib.status_string(st)}")
     return n_instr[:pop.num_exprs], slots[:pop.num_exprs]
+
+
+def compile_population(pop: Population, num_vars: int):
+    """(bytecode uint32 [n_instr, 4], instruction offsets int64 [E+1],
+    spill slots int32 [E]) exactly as the evaluator compiles the population."""
+    P = ctypes.POINTER
+    cpop = pop.as_c()
+    offs = np.zeros(pop.num_exprs + 1, np.int64)
+    slots = np.zeros(max(pop.num_exprs, 1), np.int32)
+    _lib.check(_lib.lib.sr_compile_population(ctypes.byref(cpop), num_vars, None, 0,
+                                              offs.ctypes.data_as(P(ctypes.c_int64)),
+                                              slots.ctypes.data_as(P(ctypes.c_int32))))
+    n = int(offs[-1])
+    code = np.zeros((max(n, 1), 4), np.uint32)
+    _lib.check(_lib.lib.sr_compile_population(ctypes.byref(cpop), num_vars,
+                                              code.ctypes.data_as(P(ctypes.c_uint32)), n,
+                                              offs.ctypes.data_as(P(ctypes.c_int64)),
+                                              slots.ctypes.data_as(P(ctypes.c_int32))))
+    return code[:n], offs, slots[:pop.num_exprs]

@@ -245,7 +245,8 @@ def _target(rng: np.random.Generator, X: np.ndarray, gen: TreeGen, depth: int,
         if hidden is None and len(h[0]) < 2 * depth + 1:
             continue
         yv = eval_target(h, X)
-        if np.all(np.isfinite(yv)) and np.std(yv) > 1e-6 and np.max(np.abs(yv)) < 1e6:
+        varied = X.shape[1] < 2 or np.std(yv) > 1e-6
+        if np.all(np.isfinite(yv)) and varied and np.max(np.abs(yv)) < 1e6:
             noise = rng.normal(0.0, 0.01, X.shape[1])
             return (yv + noise).astype(np.float32), h
         hidden = None
