@@ -111,7 +111,7 @@ typedef struct sr_options {
                                (MAX_CACHED_SUBTREES, cl_gpu_common.h:13)       */
   int32_t min_subtree_size; /* detection min size; reference 3 (cl_gpu_eval.cu:373) */
   int32_t min_subtree_freq; /* detection min frequency; reference 10 (same line) */
-  int32_t dpt;              /* datapoints per thread: 0 = tuned, 4 or 8        */
+  int32_t dpt;              /* datapoints per thread: 0 = tuned, 4, 8 or 16   */
   int32_t warps_per_block;  /* evaluating warps per block: 0 = tuned, 1..8     */
   int32_t autotune;         /* 1 = time candidate launch shapes on first use  */
   int32_t use_graphs;       /* 1 = replay each launch shape from a CUDA graph */

@@ -163,6 +163,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   p.dpt = dpt;
   p.W = W;
   p.smax = std::max(ps.smax, 0);
+  p.s_smem = std::min(p.smax, sr::smem_spill_slots(dpt));
   const int64_t tile = 32 * dpt;
   const int E = ps.E;
   p.G = std::max(1, W * per_warp);
@@ -172,11 +173,13 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   // Span: the target, shrunk to the data and to the shared-memory budget.
   int64_t span = std::min<int64_t>(span_target, std::max<int64_t>(tile, round_up(ctx->N, tile)));
   while (span > tile &&
-         sr::interp_smem_bytes(dpt, W, ctx->V, p.smax, static_cast<int>(span)) >
+         sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, static_cast<int>(span)) >
              static_cast<size_t>(dev_max_smem))
-    span = std::max<int64_t>(tile, span / 2);
+    span = std::max<int64_t>(tile, (span / 2) / tile * tile);
+  // The kernel walks a span tile by tile: it must hold whole tiles.
+  if (span % tile != 0) return ctx->fail(SR_ERR_UNSUPPORTED, "span is not a multiple of the tile");
   p.span = static_cast<int>(span);
-  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.smax, p.span);
+  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, p.span);
   if (p.smem > static_cast<size_t>(dev_max_smem))
     return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape needs " + std::to_string(p.smem) +
                                              " bytes of shared memory");
@@ -188,6 +191,10 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
   const int64_t resident = static_cast<int64_t>(bps) * ctx->num_sms;
   p.blocks = static_cast<int>(std::min<int64_t>(resident, std::max<int64_t>(p.items(), 1)));
+  // Global scratch for the spill slots that do not fit in shared memory.
+  const size_t spill_floats = static_cast<size_t>(p.blocks) * W *
+                              static_cast<size_t>(p.smax - p.s_smem) * static_cast<size_t>(tile);
+  if (spill_floats > 0) SR_TRY_CUDA(ctx, ctx->spill.ensure(spill_floats));
   // Group table: expressions in decreasing modelled cost, G per group, so
   // every group holds similar work and hands out its largest first.
   SR_TRY_CUDA(ctx, ps.h_group.ensure(static_cast<size_t>(std::max(p.n_groups * p.G, 1))));
@@ -251,6 +258,8 @@ sr::EvalArgs make_args(sr_context *ctx, ProgramSet &ps, int32_t *counter) {
   a.n_groups = ps.plan.n_groups;
   a.span = ps.plan.span;
   a.n_spans = ps.plan.n_spans;
+  a.spill = ctx->spill.p;
+  a.s_smem = ps.plan.s_smem;
   return a;
 }
 
@@ -293,7 +302,8 @@ void load_tune_cache(sr_context *ctx) {
         b1 == std::string::npos)
       continue;
     int dpt = 0, w = 0;
-    if (std::sscanf(line.c_str() + b0, "[%d, %d]", &dpt, &w) == 2 && (dpt == 4 || dpt == 8) &&
+    if (std::sscanf(line.c_str() + b0, "[%d, %d]", &dpt, &w) == 2 &&
+        (dpt == 4 || dpt == 8 || dpt == 16) &&
         w >= 1 && w <= sr::kMaxWarps)
       ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w};
   }
@@ -314,7 +324,7 @@ void save_tune_cache(const sr_context *ctx) {
 
 // Times each candidate shape on the prepared population and keeps the fastest.
 sr_status autotune_main(sr_context *ctx, const std::string &key) {
-  static const int kCand[][2] = {{8, 8}, {8, 12}, {8, 16}, {4, 8}, {4, 16}};
+  static const int kCand[][2] = {{16, 8}, {16, 16}, {8, 8}, {8, 16}, {4, 8}, {4, 16}};
   float best = 1e30f;
   int best_dpt = 8, best_w = 8;
   cudaEvent_t a = ctx->ev[4], b = ctx->ev[5];
@@ -420,7 +430,7 @@ sr_status sr_create(const sr_options *opts, sr_context **out) {
   sr_options o;
   if (opts) o = *opts;
   else sr_options_init(&o);
-  if (o.dpt != 0 && o.dpt != 4 && o.dpt != 8) return SR_ERR_INVALID_ARGUMENT;
+  if (o.dpt != 0 && o.dpt != 4 && o.dpt != 8 && o.dpt != 16) return SR_ERR_INVALID_ARGUMENT;
   if (o.warps_per_block < 0 || o.warps_per_block > sr::kMaxWarps) return SR_ERR_INVALID_ARGUMENT;
   if (o.cache_capacity < 0 || o.min_subtree_size < 1 || o.min_subtree_freq < 1)
     return SR_ERR_INVALID_ARGUMENT;

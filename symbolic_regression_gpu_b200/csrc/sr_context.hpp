@@ -78,6 +78,7 @@ struct Plan {
   int dpt = 8;
   int W = 8;           // evaluating warps per block
   int smax = 0;        // spill slots per warp
+  int s_smem = 0;      // of which in shared memory
   int G = 0;           // expressions per group
   int n_groups = 0;
   int span = 0;        // datapoints per span
@@ -164,6 +165,8 @@ struct sr_context {
 
   // predictions
   sr::DevBuf<float> pred;
+  // spill slots beyond the shared-memory ones (per resident warp)
+  sr::DevBuf<float> spill;
 
   // timing
   cudaEvent_t ev[6] = {};

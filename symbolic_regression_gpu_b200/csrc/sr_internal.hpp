@@ -119,6 +119,12 @@ struct EvalArgs {
   int32_t n_groups;
   int32_t span;          // datapoints per span, multiple of 32*DPT
   int32_t n_spans;
+  // Spill slots [0, s_smem) of each warp live in shared memory, slots
+  // [s_smem, smax) in this global scratch: per resident warp
+  // (blockIdx.x * W + warp), (smax - s_smem) tiles of 32*DPT floats.
+  float *spill;
+  int32_t s_smem;
+  int32_t reserved0;
 };
 
 }  // namespace sr

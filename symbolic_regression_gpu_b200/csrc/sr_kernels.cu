@@ -260,12 +260,50 @@ __device__ __forceinline__ void load_leaf(uint32_t kind, uint32_t payload, float
 }
 
 // b = operand; kind and payload are warp-uniform, kind != kBNone.
+// Spill stack of one warp: slots below s_smem in shared memory (ss), the
+// rest in global scratch (gs) written and read by the same warp only.
+struct SpillStack {
+  float *ss;
+  float *gs;
+  int s_smem;
+};
+
+template <int DPT>
+__device__ __forceinline__ void spill_store(const SpillStack &st, uint32_t slot, int lane,
+                                            const float (&T)[DPT]) {
+  constexpr int TILE = 32 * DPT;
+  if (static_cast<int>(slot) < st.s_smem)
+    sts_vec<DPT>(st.ss + slot * TILE, lane, T);
+  else
+    stg_vec<DPT>(st.gs + (slot - st.s_smem) * TILE, lane, T);
+}
+
+template <int DPT>
+__device__ __forceinline__ void spill_load(const SpillStack &st, uint32_t slot, int lane,
+                                           float (&v)[DPT]) {
+  constexpr int TILE = 32 * DPT;
+  if (static_cast<int>(slot) < st.s_smem) {
+    lds_vec<DPT>(st.ss + slot * TILE, lane, v);
+  } else {
+    // Plain (coherent) loads: the data was written by this warp in this kernel.
+    const float *base = st.gs + (slot - st.s_smem) * TILE;
+#pragma unroll
+    for (int h = 0; h < DPT / 4; ++h) {
+      const float4 q = *reinterpret_cast<const float4 *>(base + h * 128 + lane * 4);
+      v[4 * h + 0] = q.x;
+      v[4 * h + 1] = q.y;
+      v[4 * h + 2] = q.z;
+      v[4 * h + 3] = q.w;
+    }
+  }
+}
+
+// b = operand; kind and payload are warp-uniform, kind != kBNone.
 template <int DPT>
 __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, float (&b)[DPT],
-                                             const float *xs, int xrs, const float *ss,
+                                             const float *xs, int xrs, const SpillStack &st,
                                              int lane, const float *cache, int64_t ldc,
                                              int64_t dp0) {
-  constexpr int TILE = 32 * DPT;
   if (kind == kBC) {
     const float c = __uint_as_float(payload);
 #pragma unroll
@@ -275,7 +313,7 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
   } else if (kind == kBX) {
     lds_vec<DPT>(xs + payload * xrs, lane, b);
   } else {
-    lds_vec<DPT>(ss + payload * TILE, lane, b);
+    spill_load<DPT>(st, payload, lane, b);
   }
 }
 
@@ -419,31 +457,31 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
 template <int DPT>
 __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
                                             int len, const float *xs, int xrs,
-                                            float *ss, int lane, const float *cache,
-                                            int64_t ldc, int64_t dp0,
+                                            const SpillStack &st, int lane,
+                                            const float *cache, int64_t ldc, int64_t dp0,
                                             float (&T)[DPT]) {
-  constexpr int TILE = 32 * DPT;
-#pragma unroll
-  for (int k = 0; k < DPT; ++k) T[k] = 0.0f;
+  // Every program starts with an instruction that loads T.
   uint4 ins = ldg_instr(code);
   for (int i = 0; i < len; ++i) {
     // The code buffer ends with a padding instruction, so this prefetch of
     // the next word is always in bounds.
     const uint4 nxt = ldg_instr(code + i + 1);
     const uint32_t w = ins.x;
-    if (instr_spill(w)) sts_vec<DPT>(ss + instr_spill_slot(w) * TILE, lane, T);
+    if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
     if (instr_load(w))
       load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
     float b[DPT];
     const uint32_t bk = instr_b_kind(w);
-    if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, xrs, ss, lane, cache, ldc, dp0);
+    if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, xrs, st, lane, cache, ldc, dp0);
     apply_op<DPT>(instr_op(w), T, b);
     ins = nxt;
   }
 }
 
-template <int DPT, bool PRED>
-__global__ void __launch_bounds__(kMaxBlockThreads, 1) interp_kernel(const EvalArgs p) {
+// MAXW / MINB: launch bounds of the instantiation (at most MAXW evaluating
+// warps, at least MINB resident blocks per SM), which set the register budget.
+template <int DPT, bool PRED, int MAXW, int MINB>
+__global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const EvalArgs p) {
   constexpr int TILE = 32 * DPT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5;
@@ -454,7 +492,7 @@ __global__ void __launch_bounds__(kMaxBlockThreads, 1) interp_kernel(const EvalA
   float *xbuf = reinterpret_cast<float *>(smem_raw);
   float *sreg = xbuf + static_cast<size_t>(kBufs) * rows * span;
   ItemDesc *desc =
-      reinterpret_cast<ItemDesc *>(sreg + static_cast<size_t>(W) * p.smax * TILE);
+      reinterpret_cast<ItemDesc *>(sreg + static_cast<size_t>(W) * p.s_smem * TILE);
   uint64_t *full = reinterpret_cast<uint64_t *>(desc + kBufs);
   uint64_t *empty = full + kBufs;
 
@@ -510,7 +548,11 @@ __global__ void __launch_bounds__(kMaxBlockThreads, 1) interp_kernel(const EvalA
   }
 
   // ---------------- evaluating warps ----------------
-  float *ss = sreg + static_cast<size_t>(warp) * p.smax * TILE;
+  SpillStack st;
+  st.ss = sreg + static_cast<size_t>(warp) * p.s_smem * TILE;
+  st.gs = p.spill + (static_cast<size_t>(blockIdx.x) * W + warp) *
+                        static_cast<size_t>(p.smax - p.s_smem) * TILE;
+  st.s_smem = p.s_smem;
   const int tiles = span / TILE;
   uint32_t buf = 0, phase = 0;
   for (;;) {
@@ -535,23 +577,23 @@ __global__ void __launch_bounds__(kMaxBlockThreads, 1) interp_kernel(const EvalA
         if (dp0 >= p.N) break;  // tail of the last span
         const float *xs = xb + t * TILE;
         float T[DPT];
-        run_program<DPT>(code, len, xs, span, ss, lane, p.cache, p.ldc, dp0, T);
+        run_program<DPT>(code, len, xs, span, st, lane, p.cache, p.ldc, dp0, T);
         if constexpr (PRED) {
           stg_vec<DPT>(p.pred + static_cast<int64_t>(p.pred_row[e]) * p.ldp + dp0, lane, T);
         } else {
           float y[DPT];
           lds_vec<DPT>(xs + p.V * span, lane, y);
-          float sq[DPT];
+          const bool full = dp0 + TILE <= p.N;  // warp-uniform
           float s = 0.0f, c = 0.0f;  // Kahan over the lane's DPT values
           int nv = 0;
 #pragma unroll
           for (int k = 0; k < DPT; ++k) {
-            const int64_t dp = dp0 + (k / 4) * 128 + lane * 4 + (k % 4);
-            const bool valid = (dp < p.N) && isfinite(T[k]);
+            const bool valid =
+                (full || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N) && isfinite(T[k]);
             const float df = __fsub_rn(T[k], y[k]);
-            sq[k] = valid ? __fmul_rn(df, df) : 0.0f;
+            const float sq = valid ? __fmul_rn(df, df) : 0.0f;
             nv += valid ? 1 : 0;
-            const float yk = __fsub_rn(sq[k], c);
+            const float yk = __fsub_rn(sq, c);
             const float tt = __fadd_rn(s, yk);
             c = __fsub_rn(__fsub_rn(tt, s), yk);
             s = tt;
@@ -563,7 +605,12 @@ __global__ void __launch_bounds__(kMaxBlockThreads, 1) interp_kernel(const EvalA
             // when one square is infinite, like the reference's double sum.
             tile_sum = 0.0;
 #pragma unroll
-            for (int k = 0; k < DPT; ++k) tile_sum += static_cast<double>(sq[k]);
+            for (int k = 0; k < DPT; ++k) {
+              const bool valid =
+                  (full || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N) && isfinite(T[k]);
+              const float df = __fsub_rn(T[k], y[k]);
+              tile_sum += valid ? static_cast<double>(__fmul_rn(df, df)) : 0.0;
+            }
           }
           acc += tile_sum;
           cnt += nv;
@@ -714,28 +761,41 @@ __global__ void mufu_pipe_kernel(float *out, int iters) {
 
 }  // namespace
 
-size_t interp_smem_bytes(int dpt, int W, int V, int smax, int span) {
+size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span) {
   const size_t tile = 32u * static_cast<size_t>(dpt);
   return (static_cast<size_t>(kBufs) * (V + 1) * span +
-          static_cast<size_t>(W) * smax * tile) * sizeof(float) +
+          static_cast<size_t>(W) * s_smem * tile) * sizeof(float) +
          kBufs * sizeof(ItemDesc) + 2 * kBufs * sizeof(uint64_t);
 }
 
-template <int DPT, bool PRED>
+template <int DPT, bool PRED, int MAXW, int MINB>
 static const void *interp_fn() {
-  return reinterpret_cast<const void *>(&interp_kernel<DPT, PRED>);
+  return reinterpret_cast<const void *>(&interp_kernel<DPT, PRED, MAXW, MINB>);
 }
 
-static const void *select_interp(int dpt, bool pred) {
-  if (dpt == 8) return pred ? interp_fn<8, true>() : interp_fn<8, false>();
-  if (dpt == 4) return pred ? interp_fn<4, true>() : interp_fn<4, false>();
+// Instantiations: W <= 8 uses the narrow variants (more blocks per SM, tighter
+// register budget), larger W the wide ones.
+static const void *select_interp(int dpt, bool pred, int W) {
+  const bool narrow = W <= 8;
+  if (dpt == 16) {
+    if (narrow) return pred ? interp_fn<16, true, 8, 2>() : interp_fn<16, false, 8, 2>();
+    return pred ? interp_fn<16, true, 16, 1>() : interp_fn<16, false, 16, 1>();
+  }
+  if (dpt == 8) {
+    if (narrow) return pred ? interp_fn<8, true, 8, 3>() : interp_fn<8, false, 8, 3>();
+    return pred ? interp_fn<8, true, 16, 1>() : interp_fn<8, false, 16, 1>();
+  }
+  if (dpt == 4) {
+    if (narrow) return pred ? interp_fn<4, true, 8, 4>() : interp_fn<4, false, 8, 4>();
+    return pred ? interp_fn<4, true, 16, 2>() : interp_fn<4, false, 16, 2>();
+  }
   return nullptr;
 }
 
 cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
                              int *blocks_per_sm) {
-  const void *fn = select_interp(dpt, pred);
-  if (!fn) return cudaErrorInvalidValue;
+  const void *fn = select_interp(dpt, pred, W);
+  if (!fn || W < 1 || W > kMaxWarps) return cudaErrorInvalidValue;
   cudaError_t err = cudaFuncSetAttribute(
       fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (err != cudaSuccess) return err;
@@ -745,21 +805,10 @@ cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
 
 cudaError_t launch_interp(int dpt, bool pred, const EvalArgs &args, int blocks,
                           size_t smem, cudaStream_t stream) {
-  const dim3 grid(blocks), block((args.W + 1) * 32);
-  if (dpt == 8) {
-    if (pred)
-      interp_kernel<8, true><<<grid, block, smem, stream>>>(args);
-    else
-      interp_kernel<8, false><<<grid, block, smem, stream>>>(args);
-  } else if (dpt == 4) {
-    if (pred)
-      interp_kernel<4, true><<<grid, block, smem, stream>>>(args);
-    else
-      interp_kernel<4, false><<<grid, block, smem, stream>>>(args);
-  } else {
-    return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
+  const void *fn = select_interp(dpt, pred, args.W);
+  if (!fn || args.W < 1 || args.W > kMaxWarps) return cudaErrorInvalidValue;
+  void *params[] = {const_cast<EvalArgs *>(&args)};
+  return cudaLaunchKernel(fn, dim3(blocks), dim3((args.W + 1) * 32), params, smem, stream);
 }
 
 cudaError_t launch_finalize(const double2 *partial, int n_spans, int E,

@@ -14,7 +14,10 @@ constexpr int64_t kDataAlign = 4096;               // X / cache row stride multi
 constexpr int kPlainStack = 128;                    // plain kernel stack depth
 
 // Dynamic shared memory of interp_kernel for a launch shape.
-size_t interp_smem_bytes(int dpt, int W, int V, int smax, int span);
+size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span);
+// Spill slots per warp kept in shared memory for a datapoints-per-thread
+// choice (deeper slots go to global scratch).
+inline int smem_spill_slots(int dpt) { return dpt >= 16 ? 2 : (dpt == 8 ? 4 : 8); }
 // Sets the dynamic-smem attribute and returns resident blocks per SM.
 cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
                              int *blocks_per_sm);
