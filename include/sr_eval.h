@@ -302,6 +302,33 @@ sr_status sr_compile_population(const sr_population *pop, int32_t num_vars, uint
                                 int64_t code_capacity, int64_t *instr_offsets,
                                 int32_t *spill_slots);
 
+/* ---- evaluation without any device allocation (no counterpart in the
+ *      reference) ------------------------------------------------------------
+ * For callers that keep their population on the GPU and cannot let a library
+ * call cudaMalloc: a GA loop that breeds and evaluates on the device inside a
+ * fixed memory budget, or a host framework whose own pooled allocator owns
+ * all device memory.  Every argument is a device pointer the caller owns:
+ * tokens / values (float: the constant, or the variable index as a number) /
+ * offsets (num_exprs + 1, int64) describe the population in the layout of
+ * sr_population, X is column-major with row stride ld (y in row num_vars),
+ * mse_out receives num_exprs floats.  The plain per-expression kernel does
+ * the work; its partial sums live in one fixed array built into the
+ * library (SR_NOALLOC_SCRATCH_BYTES, resident on every GPU that loads the
+ * library until exit), so no call allocates.  The first call on a device
+ * looks up that array's device address (one-time set-up; make that first
+ * call before any stream capture).  The call runs on `stream` (NULL = the
+ * default stream) and waits for it before returning.  Calls share the
+ * array: calls whose kernels overlap on the GPU race and their results are
+ * undefined.  Expressions are validated on the device: a malformed one gets
+ * a NaN MSE and the call returns SR_ERR_MALFORMED_EXPRESSION.  num_exprs >
+ * SR_NOALLOC_MAX_EXPRS returns SR_ERR_UNSUPPORTED. */
+#define SR_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define SR_NOALLOC_MAX_EXPRS ((int32_t)((SR_NOALLOC_SCRATCH_BYTES - 256u) / 16u))
+sr_status sr_eval_mse_device_noalloc(const int32_t *tokens, const float *values,
+                                     const int64_t *offsets, int32_t num_exprs, const float *X,
+                                     int64_t ld, int32_t num_vars, int64_t num_dps,
+                                     float *mse_out, void *stream);
+
 /* ---- misc ------------------------------------------------------------------ */
 sr_status sr_get_stream(sr_context *ctx, void **stream);
 sr_status sr_synchronize(sr_context *ctx);

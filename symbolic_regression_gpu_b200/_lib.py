@@ -36,6 +36,10 @@ SR_EVAL_SUBTREE_CACHE = 0x1
 SR_EVAL_CLEAR_CACHE = 0x2
 SR_EVAL_PLAIN = 0x4
 
+# bounds of sr_eval_mse_device_noalloc (include/sr_eval.h)
+SR_NOALLOC_SCRATCH_BYTES = 4 << 20
+SR_NOALLOC_MAX_EXPRS = (SR_NOALLOC_SCRATCH_BYTES - 256) // 16
+
 SR_GRAD_RECOMPUTE = 0
 SR_GRAD_CHECKPOINT = 1
 
@@ -154,6 +158,8 @@ _SIGNATURES = {
                                          _P(c_int32)]),
     "sr_compile_population": (c_int32, [_P(sr_population), c_int32, _P(c_uint32), c_int64,
                                         _P(c_int64), _P(c_int32)]),
+    "sr_eval_mse_device_noalloc": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
+                                             c_int64, c_int32, c_int64, c_void_p, c_void_p]),
     "sr_get_stream": (c_int32, [c_void_p, _P(c_void_p)]),
     "sr_synchronize": (c_int32, [c_void_p]),
     "sr_measure_pipes": (c_int32, [c_void_p, _P(c_double), _P(c_double), _P(c_int32)]),
