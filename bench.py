@@ -48,6 +48,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-baseline", action="store_true",
                     help="also time the plain per-expression kernel")
+    ap.add_argument("--exprs", type=int, default=0,
+                    help="population size override (profiling cases)")
+    ap.add_argument("--dpt", type=int, default=0, help="force datapoints per thread")
+    ap.add_argument("--warps", type=int, default=0, help="force evaluating warps per block")
+    ap.add_argument("--profile-launch", action="store_true",
+                    help="prepare and run a single evaluation, no timing (for ncu)")
     return ap.parse_args()
 
 
@@ -56,11 +62,30 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", "1")))
 
 
-def make_workload(name: str, rank: int):
+def make_workload(name: str, rank: int, exprs: int = 0):
     from symbolic_regression_gpu_b200 import synth
     fn = synth.WORKLOADS[name]
     seeds = {"plain": 1, "batched": 2, "cache": 3, "grad": 4, "large": 5}
-    return fn(seed=seeds[name] + 1000 * rank)
+    kw = {"E": exprs} if exprs > 0 else {}
+    return fn(seed=seeds[name] + 1000 * rank, **kw)
+
+
+def profile_launch(args):
+    """One prepared evaluation on GPU 0, nothing timed (the ncu capture case)."""
+    from symbolic_regression_gpu_b200 import Evaluator
+    w = make_workload(args.workload, 0, args.exprs)
+    with Evaluator(device=0, dpt=args.dpt, warps_per_block=args.warps) as ev:
+        ev.set_data(w.X)
+        ev.prepare(w.population)
+        ev.launch()
+        mse = ev.read_mse()
+        st = ev.stats
+        print(json.dumps({"workload": w.name, "exprs": w.population.num_exprs,
+                          "num_dps": w.num_dps, "dpt": st.dpt,
+                          "warps_per_block": st.warps_per_block, "blocks": st.blocks,
+                          "work_items": st.work_items, "kernel_ms": st.eval_kernel_time_ms,
+                          "finite_mse": int(np.isfinite(mse).sum())}))
+    return 0
 
 
 def config_of(w, world: int, flush: str):
@@ -176,7 +201,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/libref_oracle.so was not built"}))
         return 0
-    w = make_workload(args.workload, 0)
+    w = make_workload(args.workload, 0, args.exprs)
     threads = os.cpu_count() or 1
     pop = _reference_population(w.population)
     E = pop.num_exprs
@@ -231,10 +256,11 @@ def run_ours(args):
 
     from symbolic_regression_gpu_b200 import Evaluator
 
-    w = make_workload(args.workload, rank)
+    w = make_workload(args.workload, rank, args.exprs)
     flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     tune_path = os.path.join("/tmp", f"sr_tune_{os.getuid()}.json")
-    ev = Evaluator(device=local_rank, autotune=True, tune_cache_path=tune_path)
+    ev = Evaluator(device=local_rank, autotune=True, tune_cache_path=tune_path, dpt=args.dpt,
+                   warps_per_block=args.warps)
     sr_stream = torch.cuda.ExternalStream(ev.stream_handle, device=dev)
     ev.set_data(w.X)
     ev.prepare(w.population)  # compile + upload + shape tuning (outside timing)
@@ -379,6 +405,8 @@ def run_ours(args):
 
 def main():
     args = parse_args()
+    if args.profile_launch:
+        return profile_launch(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
