@@ -48,6 +48,9 @@ def _load_oracle():
     lib.sro_mse_f32.argtypes = [c_int, _I32, _F64, _I64, c_int, c_int64, _F32, _F32, c_int]
     lib.sro_mse_f64.restype = None
     lib.sro_mse_f64.argtypes = [c_int, _I32, _F64, _I64, c_int, c_int64, _F32, _F64, _I64, c_int]
+    lib.sro_grad_f64.restype = None
+    lib.sro_grad_f64.argtypes = [c_int, _I32, _F64, _I64, c_int, c_int64, _F32, _F64, _F64,
+                                 _F64, c_int]
     lib.sro_flat_key.restype = c_uint64
     lib.sro_flat_key.argtypes = [_I32, _F64, c_int]
     lib.sro_merkle.restype = None
@@ -143,6 +146,24 @@ def mse_f64(pop, X: np.ndarray, threads: int = 0):
     _oracle.sro_mse_f64(pop.num_exprs, _p(t, _I32), _p(v, _F64), _p(o, _I64), V, N,
                         _p(X, _F32), _p(out, _F64), _p(cnt, _I64), threads or os.cpu_count())
     return out, cnt
+
+
+def grad_f64(pop, X: np.ndarray, threads: int = 0, with_abs: bool = False):
+    """(FP64 MSE [E], FP64 d MSE / d constants [C], constants in token order);
+    with_abs adds the mean absolute per-datapoint contribution [C]."""
+    t, v, o = _pop_arrays(pop)
+    X = np.ascontiguousarray(X, np.float32)
+    V, N = X.shape[0] - 1, X.shape[1]
+    mse = np.empty(pop.num_exprs, np.float64)
+    C = int(np.count_nonzero(t == 0))
+    grad = np.empty(max(C, 1), np.float64)
+    gabs = np.empty(max(C, 1), np.float64) if with_abs else None
+    _oracle.sro_grad_f64(pop.num_exprs, _p(t, _I32), _p(v, _F64), _p(o, _I64), V, N,
+                         _p(X, _F32), _p(mse, _F64), _p(grad, _F64),
+                         _p(gabs, _F64) if with_abs else None, threads or os.cpu_count())
+    if with_abs:
+        return mse, grad[:C], gabs[:C]
+    return mse, grad[:C]
 
 
 def mse_of_predictions(pred: np.ndarray, y: np.ndarray) -> np.ndarray:

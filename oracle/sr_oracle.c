@@ -306,3 +306,170 @@ void sro_merkle(const int32_t *tok, const double *val, int len, int32_t *sizes,
     hashes[i] = h;
   }
 }
+
+/* ---- FP64 gradient of the MSE with respect to the constants --------------
+ * No reference counterpart (the reference has no gradient).  Reverse mode on
+ * the expression tree in double: values bottom-up, adjoints top-down in
+ * prefix order (a parent precedes its children).  Derivative conventions at
+ * non-smooth points match the device adjoint: |x|, sqrt|x|, LOOSE_LOG have
+ * derivative 0 at 0; the protected regions of LOOSE_DIV / LOOSE_INV and the
+ * exp clamp (x >= 80) have derivative 0; MIN / MAX route to the returned
+ * operand (the first on ties, the non-NaN one); 0^0 of LOOSE_POW has
+ * derivative 0; a zero adjoint times any partial is zero.  A datapoint
+ * counts when its FP64 prediction would be a finite float. */
+static double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+static double strong(double g, double d) { return g == 0.0 ? 0.0 : g * d; }
+
+typedef struct {
+  int E, V;
+  int64_t N;
+  const int32_t *tok;
+  const double *val;
+  const int64_t *off;
+  const float *X;
+  double *mse;
+  double *grad;
+  double *gabs;
+  int e0, e1;
+} sro_gjob;
+
+static void *sro_grad_worker(void *arg) {
+  sro_gjob *j = (sro_gjob *)arg;
+  const int V = j->V;
+  const float *y = j->X + (int64_t)V * j->N;
+  for (int e = j->e0; e < j->e1; ++e) {
+    const int32_t *t = j->tok + j->off[e];
+    const double *vl = j->val + j->off[e];
+    const int L = (int)(j->off[e + 1] - j->off[e]);
+    int size[SRO_STACK], cidx[SRO_STACK];
+    double v[SRO_STACK], adj[SRO_STACK];
+    int nc = 0;
+    for (int i = 0; i < L; ++i) cidx[i] = (t[i] == 0) ? nc++ : -1;
+    /* constants of this expression start at its CSR offset */
+    int64_t cbase = 0;
+    for (int64_t q = 0; q < j->off[e]; ++q) cbase += (j->tok[q] == 0);
+    double *g = j->grad + cbase;
+    double *ga = j->gabs ? j->gabs + cbase : NULL;
+    for (int c = 0; c < nc; ++c) g[c] = 0.0;
+    if (ga)
+      for (int c = 0; c < nc; ++c) ga[c] = 0.0;
+    for (int i = L - 1; i >= 0; --i) {
+      if (t[i] <= 0) { size[i] = 1; continue; }
+      int s = 1, pos = i + 1, ar = (t[i] >= 1 && t[i] <= 9) ? 2 : 1;
+      for (int k = 0; k < ar && pos < L; ++k) { s += size[pos]; pos += size[pos]; }
+      size[i] = s;
+    }
+    double sum = 0.0;
+    int64_t count = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int64_t dp = 0; dp < j->N; ++dp) {
+        for (int i = L - 1; i >= 0; --i) {
+          const int tk = t[i];
+          if (tk == 0) { v[i] = (double)(float)vl[i]; continue; }
+          if (tk == -1) {
+            const int vi = var_index(vl[i]);
+            v[i] = (vi >= 0 && vi < V) ? (double)j->X[(int64_t)vi * j->N + dp] : 0.0;
+            continue;
+          }
+          const double a = v[i + 1];
+          const double b = (tk >= 1 && tk <= 9) ? v[i + 1 + size[i + 1]] : 0.0;
+          v[i] = sro_op_f64(tk, a, b);
+        }
+        const double p = v[0];
+        if (isnan(p) || isinf((float)p)) continue;
+        const double d = p - (double)y[dp];
+        if (pass == 0) { sum += d * d; ++count; continue; }
+        for (int i = 0; i < L; ++i) adj[i] = 0.0;
+        adj[0] = 2.0 * d;
+        for (int i = 0; i < L; ++i) {
+          const int tk = t[i];
+          const double gi = adj[i];
+          if (tk == 0) {
+            g[cidx[i]] += gi;
+            if (ga) ga[cidx[i]] += fabs(gi);
+            continue;
+          }
+          if (tk == -1) continue;
+          const int l = i + 1;
+          const double a = v[l], out = v[i];
+          if (tk >= 1 && tk <= 9) {
+            const int r = l + size[l];
+            const double b = v[r];
+            double da = 0, db = 0;
+            switch (tk) {
+              case 1: da = 1; db = 1; break;
+              case 2: da = 1; db = -1; break;
+              case 3: da = b; db = a; break;
+              case 4: da = 1.0 / b; db = -out / b; break;
+              case 5: da = b * pow(a, b - 1.0); db = out * log(a); break;
+              case 6: { const int first = isnan(b) || (!isnan(a) && a <= b); da = first; db = !first; } break;
+              case 7: { const int first = isnan(b) || (!isnan(a) && a >= b); da = first; db = !first; } break;
+              case 8: {
+                const double den = fabs(b) <= 1e-9 ? (b < 0 ? -1e-9 : 1e-9) : b;
+                da = 1.0 / den;
+                db = fabs(b) <= 1e-9 ? 0.0 : -out / den;
+              } break;
+              case 9: {
+                const int z = (a == 0.0 && b == 0.0);
+                da = z ? 0.0 : b * pow(fabs(a), b - 1.0) * sgn(a);
+                db = z ? 0.0 : out * log(fabs(a));
+              } break;
+            }
+            adj[l] += strong(gi, da);
+            adj[r] += strong(gi, db);
+          } else {
+            double da = 0;
+            switch (tk) {
+              case 10: da = cos(a); break;
+              case 11: da = -sin(a); break;
+              case 12: da = 1.0 + out * out; break;
+              case 13: da = cosh(a); break;
+              case 14: da = sinh(a); break;
+              case 15: da = 1.0 - out * out; break;
+              case 16: da = out; break;
+              case 17: da = 1.0 / a; break;
+              case 18: da = -out * out; break;
+              case 19: da = 1.0 / sqrt(1.0 - a * a); break;
+              case 20: da = -1.0 / sqrt(1.0 - a * a); break;
+              case 21: da = 1.0 / (1.0 + a * a); break;
+              case 22: da = (a == 0.0) ? 0.0 : 1.0 / a; break;
+              case 23: da = fabs(a) <= 1e-9 ? 0.0 : -out * out; break;
+              case 24: da = sgn(a); break;
+              case 25: da = -1; break;
+              case 26: da = 0.5 / out; break;
+              case 27: da = (a == 0.0) ? 0.0 : sgn(a) * 0.5 / out; break;
+              case 32: da = (a < 80.0) ? out : 0.0; break;
+            }
+            adj[l] += strong(gi, da);
+          }
+        }
+      }
+    }
+    j->mse[e] = count > 0 ? sum / (double)count : NAN;
+    for (int c = 0; c < nc; ++c) g[c] = count > 0 ? g[c] / (double)count : NAN;
+    if (ga)
+      for (int c = 0; c < nc; ++c) ga[c] = count > 0 ? ga[c] / (double)count : NAN;
+  }
+  return NULL;
+}
+
+/* mse [E] and grad [C] (constants in token order, CSR over expressions);
+ * gabs [C] (may be NULL) = mean over valid datapoints of |adjoint reaching
+ * each constant occurrence|, the scale of the summation's rounding error. */
+void sro_grad_f64(int E, const int32_t *tok, const double *val, const int64_t *off,
+                  int num_vars, int64_t N, const float *X, double *mse, double *grad,
+                  double *gabs, int threads) {
+  if (threads < 1) threads = 1;
+  if (threads > 256) threads = 256;
+  if (threads > E) threads = E > 0 ? E : 1;
+  pthread_t th[256];
+  sro_gjob jobs[256];
+  for (int k = 0; k < threads; ++k) {
+    sro_gjob jb = {E, num_vars, N, tok, val, off, X, mse, grad, gabs,
+                   (int)((int64_t)E * k / threads), (int)((int64_t)E * (k + 1) / threads)};
+    jobs[k] = jb;
+  }
+  for (int k = 1; k < threads; ++k) pthread_create(&th[k], NULL, sro_grad_worker, &jobs[k]);
+  sro_grad_worker(&jobs[0]);
+  for (int k = 1; k < threads; ++k) pthread_join(th[k], NULL);
+}

@@ -101,6 +101,7 @@ struct ProgramSet {
   PinnedBuf<int32_t> h_group;
   PinnedBuf<int32_t> h_row;
   std::vector<float> cost;  // per expression
+  std::vector<int32_t> n_const;  // constants per expression
   int E = 0;
   int smax = 0;
   int64_t n_instr = 0;
@@ -122,6 +123,36 @@ struct PlainSet {
   PinnedBuf<int32_t> h_len;
   int E = 0;
   int n_dpblocks = 0;
+};
+
+// One launch of the forward+adjoint kernel: expressions whose programs fit
+// the class's tape length.
+struct AdjClass {
+  int tape_len = 0;
+  int gmax = 0;
+  int64_t group_off = 0;  // into the concatenated group table
+  Plan plan;
+};
+
+// Device state of a gradient / constant-optimisation call.
+struct GradSet {
+  DevBuf<int64_t> const_off;
+  DevBuf<int32_t> const_cnt;
+  DevBuf<int64_t> const_loc;  // (instruction << 1) | (operand b)
+  DevBuf<double> grad_acc;
+  DevBuf<float> grad;
+  DevBuf<float> consts;
+  DevBuf<float> m, v;
+  DevBuf<int32_t> groups;
+  PinnedBuf<int64_t> h_const_off;
+  PinnedBuf<int32_t> h_const_cnt;
+  PinnedBuf<int64_t> h_const_loc;
+  PinnedBuf<float> h_consts;
+  PinnedBuf<int32_t> h_groups;
+  std::vector<AdjClass> classes;
+  int64_t C = 0;
+  int span = 0;
+  int n_spans = 0;
 };
 
 enum class Mode { kNone, kBatched, kCached, kPlain };
@@ -167,6 +198,8 @@ struct sr_context {
   sr::DevBuf<float> pred;
   // spill slots beyond the shared-memory ones (per resident warp)
   sr::DevBuf<float> spill;
+  // gradients / constant optimisation
+  sr::GradSet grad;
 
   // timing
   cudaEvent_t ev[6] = {};

@@ -32,7 +32,10 @@
 //   Instr.a  payload of leaf A, Instr.b payload of operand b: spill slot /
 //            variable row / float bits of the constant / cache slot
 //   Instr.c  bits 0..9 / 10..19: constant index (token order) of leaf A /
-//            operand b when it is a constant, 0x3FF otherwise (adjoint).
+//            operand b when it is a constant, 0x3FF otherwise; bits 20..29:
+//            when b is a spill slot, the program-relative index of the
+//            instruction whose output was spilled there (the adjoint reads
+//            that value back from its tape).
 #pragma once
 #include <cstdint>
 #include <vector_types.h>

@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "sr_device.cuh"
 #include "sr_eval.h"
 #include "sr_internal.hpp"
 #include "sr_kernels.hpp"
@@ -36,447 +37,6 @@
 namespace sr {
 
 namespace {
-
-constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s per mbarrier wait
-constexpr uint64_t kDrainLimitNs = 100000000ull;  // 100 ms on error paths
-
-struct alignas(16) ItemDesc {
-  int32_t item;   // work item, -1 = no more work
-  int32_t group;
-  int32_t span;
-  int32_t claim;  // next expression of the group to hand out
-};
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ uint64_t global_timer_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(count)
-               : "memory");
-}
-
-__device__ __forceinline__ void mbar_init_fence() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar,
-                                                      uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                   smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n"
-      "  .reg .pred p;\n"
-      "  mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      "  selp.u32 %0, 1, 0, p;\n"
-      "}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: gives up after kWaitLimitNs (sets kDevErrTimeout) or as soon
-// as another warp has flagged an error.  Never spins forever.
-__device__ __noinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
-                                       int32_t *err) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_timer_ns();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63u) == 0) {
-      if (*reinterpret_cast<volatile int32_t *>(err) != 0) return false;
-      if (global_timer_ns() - t0 > kWaitLimitNs) {
-        atomicOr(err, kDevErrTimeout);
-        return false;
-      }
-    }
-  }
-}
-
-// Wait used only while draining copies on an error path.
-__device__ __noinline__ void mbar_drain(uint64_t *bar, uint32_t parity) {
-  const uint64_t t0 = global_timer_ns();
-  while (!mbar_try_wait(bar, parity)) {
-    if (global_timer_ns() - t0 > kDrainLimitNs) return;
-  }
-}
-
-// Bulk copy global -> shared (no multicast), completion counted on `bar`.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
-                                         uint32_t bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-      "[%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ uint4 ldg_instr(const Instr *p) {
-  return __ldg(reinterpret_cast<const uint4 *>(p));
-}
-
-// Datapoint layout inside a tile of 32*DPT: element k of lane l is datapoint
-// (k/4)*128 + 4*l + (k%4), so every vector access of a warp covers 512
-// contiguous bytes (conflict-free in shared memory, coalesced in global).
-template <int DPT>
-__device__ __forceinline__ void lds_vec(const float *base, int lane,
-                                        float (&v)[DPT]) {
-#pragma unroll
-  for (int h = 0; h < DPT / 4; ++h) {
-    const float4 q = *reinterpret_cast<const float4 *>(base + h * 128 + lane * 4);
-    v[4 * h + 0] = q.x;
-    v[4 * h + 1] = q.y;
-    v[4 * h + 2] = q.z;
-    v[4 * h + 3] = q.w;
-  }
-}
-
-template <int DPT>
-__device__ __forceinline__ void sts_vec(float *base, int lane,
-                                        const float (&v)[DPT]) {
-#pragma unroll
-  for (int h = 0; h < DPT / 4; ++h)
-    *reinterpret_cast<float4 *>(base + h * 128 + lane * 4) =
-        make_float4(v[4 * h + 0], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
-}
-
-template <int DPT>
-__device__ __forceinline__ void ldg_vec(const float *base, int lane,
-                                        float (&v)[DPT]) {
-#pragma unroll
-  for (int h = 0; h < DPT / 4; ++h) {
-    const float4 q = __ldg(reinterpret_cast<const float4 *>(base + h * 128 + lane * 4));
-    v[4 * h + 0] = q.x;
-    v[4 * h + 1] = q.y;
-    v[4 * h + 2] = q.z;
-    v[4 * h + 3] = q.w;
-  }
-}
-
-template <int DPT>
-__device__ __forceinline__ void stg_vec(float *base, int lane,
-                                        const float (&v)[DPT]) {
-#pragma unroll
-  for (int h = 0; h < DPT / 4; ++h)
-    *reinterpret_cast<float4 *>(base + h * 128 + lane * 4) =
-        make_float4(v[4 * h + 0], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
-}
-
-// ---- out-of-line 4-wide operator routines ---------------------------------
-// Every routine that expands to more than a handful of instructions (CUDA's
-// accurate transcendentals, IEEE division / reciprocal / square root, powf)
-// exists once, four datapoints wide, instead of being inlined DPT times into
-// each opcode of the dispatch switch: that keeps the interpreter's code small
-// enough for the instruction cache.
-#ifndef SR_INLINE_MATH
-#define SR_INLINE_MATH 0
-#endif
-#if SR_INLINE_MATH
-#define SR_OUTLINE __forceinline__
-#else
-#define SR_OUTLINE __noinline__
-#endif
-#define SR_V1(NAME, EXPR)                                                   \
-  __device__ SR_OUTLINE float4 NAME(float4 v) {                             \
-    float4 r;                                                               \
-    { const float x = v.x; r.x = (EXPR); }                                  \
-    { const float x = v.y; r.y = (EXPR); }                                  \
-    { const float x = v.z; r.z = (EXPR); }                                  \
-    { const float x = v.w; r.w = (EXPR); }                                  \
-    return r;                                                               \
-  }
-#define SR_V2(NAME, EXPR)                                                   \
-  __device__ SR_OUTLINE float4 NAME(float4 u, float4 v) {                   \
-    float4 r;                                                               \
-    { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
-    { const float x = u.y, y = v.y; r.y = (EXPR); }                         \
-    { const float x = u.z, y = v.z; r.z = (EXPR); }                         \
-    { const float x = u.w, y = v.w; r.w = (EXPR); }                         \
-    return r;                                                               \
-  }
-SR_V1(v_sin, sinf(x))
-SR_V1(v_cos, cosf(x))
-SR_V1(v_tan, tanf(x))
-SR_V1(v_sinh, sinhf(x))
-SR_V1(v_cosh, coshf(x))
-SR_V1(v_tanh, tanhf(x))
-SR_V1(v_exp, expf(x))
-SR_V1(v_log, logf(x))
-SR_V1(v_asin, asinf(x))
-SR_V1(v_acos, acosf(x))
-SR_V1(v_atan, atanf(x))
-SR_V1(v_rcp, __frcp_rn(x))
-SR_V1(v_sqrt, __fsqrt_rn(x))
-SR_V2(v_div, __fdiv_rn(x, y))
-SR_V2(v_pow, powf(x, y))
-#undef SR_V1
-#undef SR_V2
-
-template <int DPT>
-__device__ __forceinline__ float4 quad(const float (&v)[DPT], int h) {
-  return make_float4(v[4 * h + 0], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
-}
-template <int DPT>
-__device__ __forceinline__ void unquad(float (&v)[DPT], int h, float4 q) {
-  v[4 * h + 0] = q.x;
-  v[4 * h + 1] = q.y;
-  v[4 * h + 2] = q.z;
-  v[4 * h + 3] = q.w;
-}
-
-// T = leaf; kind and payload are warp-uniform.
-template <int DPT>
-__device__ __forceinline__ void load_leaf(uint32_t kind, uint32_t payload, float (&T)[DPT],
-                                          const float *xs, int xrs, int lane,
-                                          const float *cache, int64_t ldc, int64_t dp0) {
-  if (kind == kLeafX) {
-    lds_vec<DPT>(xs + payload * xrs, lane, T);
-  } else if (kind == kLeafC) {
-    const float c = __uint_as_float(payload);
-#pragma unroll
-    for (int k = 0; k < DPT; ++k) T[k] = c;
-  } else {
-    ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, T);
-  }
-}
-
-// b = operand; kind and payload are warp-uniform, kind != kBNone.
-// Spill stack of one warp: slots below s_smem in shared memory (ss), the
-// rest in global scratch (gs) written and read by the same warp only.
-struct SpillStack {
-  float *ss;
-  float *gs;
-  int s_smem;
-};
-
-template <int DPT>
-__device__ __forceinline__ void spill_store(const SpillStack &st, uint32_t slot, int lane,
-                                            const float (&T)[DPT]) {
-  constexpr int TILE = 32 * DPT;
-  if (static_cast<int>(slot) < st.s_smem)
-    sts_vec<DPT>(st.ss + slot * TILE, lane, T);
-  else
-    stg_vec<DPT>(st.gs + (slot - st.s_smem) * TILE, lane, T);
-}
-
-template <int DPT>
-__device__ __forceinline__ void spill_load(const SpillStack &st, uint32_t slot, int lane,
-                                           float (&v)[DPT]) {
-  constexpr int TILE = 32 * DPT;
-  if (static_cast<int>(slot) < st.s_smem) {
-    lds_vec<DPT>(st.ss + slot * TILE, lane, v);
-  } else {
-    // Plain (coherent) loads: the data was written by this warp in this kernel.
-    const float *base = st.gs + (slot - st.s_smem) * TILE;
-#pragma unroll
-    for (int h = 0; h < DPT / 4; ++h) {
-      const float4 q = *reinterpret_cast<const float4 *>(base + h * 128 + lane * 4);
-      v[4 * h + 0] = q.x;
-      v[4 * h + 1] = q.y;
-      v[4 * h + 2] = q.z;
-      v[4 * h + 3] = q.w;
-    }
-  }
-}
-
-// b = operand; kind and payload are warp-uniform, kind != kBNone.
-template <int DPT>
-__device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, float (&b)[DPT],
-                                             const float *xs, int xrs, const SpillStack &st,
-                                             int lane, const float *cache, int64_t ldc,
-                                             int64_t dp0) {
-  if (kind == kBC) {
-    const float c = __uint_as_float(payload);
-#pragma unroll
-    for (int k = 0; k < DPT; ++k) b[k] = c;
-  } else if (kind == kBR) {
-    ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, b);
-  } else if (kind == kBX) {
-    lds_vec<DPT>(xs + payload * xrs, lane, b);
-  } else {
-    spill_load<DPT>(st, payload, lane, b);
-  }
-}
-
-#define SR_EACH(STMT)                                            \
-  {                                                              \
-    _Pragma("unroll") for (int k = 0; k < DPT; ++k) { STMT; }   \
-  }                                                              \
-  break;
-#define SR_CALL1(FN)                                                      \
-  {                                                                       \
-    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h)                   \
-        unquad<DPT>(T, h, FN(quad<DPT>(T, h)));                           \
-  }                                                                       \
-  break;
-#define SR_CALL2(FN, X, Y)                                                \
-  {                                                                       \
-    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h)                   \
-        unquad<DPT>(T, h, FN(quad<DPT>(X, h), quad<DPT>(Y, h)));          \
-  }                                                                       \
-  break;
-
-// T = op(T, b) (T = op(T) for unary operators) for DPT datapoints; the
-// switch is on a warp-uniform opcode.  Semantics: sr_ops.cuh.
-template <int DPT>
-__device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b)[DPT]) {
-  const float kNaN = qnan();
-  switch (op) {
-    case 0: break;
-    case 1: SR_EACH(T[k] = __fadd_rn(T[k], b[k]))
-    case 2: SR_EACH(T[k] = __fsub_rn(T[k], b[k]))
-    case 42: SR_EACH(T[k] = __fsub_rn(b[k], T[k]))
-    case 3: SR_EACH(T[k] = __fmul_rn(T[k], b[k]))
-    case 4: {  // DIV: NaN when the divisor is 0
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_div(quad<DPT>(T, h), quad<DPT>(b, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = (b[k] == 0.0f) ? kNaN : T[k];
-    } break;
-    case 44: {  // reversed DIV: b / T
-      float den[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) den[k] = T[k];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_div(quad<DPT>(b, h), quad<DPT>(den, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = (den[k] == 0.0f) ? kNaN : T[k];
-    } break;
-    case 5: SR_CALL2(v_pow, T, b)
-    case 45: SR_CALL2(v_pow, b, T)
-    case 6: SR_EACH(T[k] = fminf(T[k], b[k]))
-    case 46: SR_EACH(T[k] = fminf(b[k], T[k]))
-    case 7: SR_EACH(T[k] = fmaxf(T[k], b[k]))
-    case 47: SR_EACH(T[k] = fmaxf(b[k], T[k]))
-    case 8: {  // LOOSE_DIV: T / protected(b)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) b[k] = loose_denom(b[k]);
-    }
-      SR_CALL2(v_div, T, b)
-    case 48: {  // reversed LOOSE_DIV: b / protected(T)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = loose_denom(T[k]);
-    }
-      SR_CALL2(v_div, b, T)
-    case 9: {  // LOOSE_POW: 0^0 = 0, else |T|^b
-      bool z[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        z[k] = (T[k] == 0.0f && b[k] == 0.0f);
-        T[k] = fabsf(T[k]);
-      }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_pow(quad<DPT>(T, h), quad<DPT>(b, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = z[k] ? 0.0f : T[k];
-    } break;
-    case 49: {  // reversed LOOSE_POW: 0^0 = 0, else |b|^T
-      bool z[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        z[k] = (T[k] == 0.0f && b[k] == 0.0f);
-        b[k] = fabsf(b[k]);
-      }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_pow(quad<DPT>(b, h), quad<DPT>(T, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = z[k] ? 0.0f : T[k];
-    } break;
-    case 10: SR_CALL1(v_sin)
-    case 11: SR_CALL1(v_cos)
-    case 12: SR_CALL1(v_tan)
-    case 13: SR_CALL1(v_sinh)
-    case 14: SR_CALL1(v_cosh)
-    case 15: SR_CALL1(v_tanh)
-    case 16: SR_CALL1(v_exp)
-    case 17: SR_CALL1(v_log)
-    case 18: SR_CALL1(v_rcp)
-    case 19: SR_CALL1(v_asin)
-    case 20: SR_CALL1(v_acos)
-    case 21: SR_CALL1(v_atan)
-    case 22: {  // LOOSE_LOG: -1e9 at 0, else log|T|
-      bool z[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        z[k] = (T[k] == 0.0f);
-        T[k] = fabsf(T[k]);
-      }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_log(quad<DPT>(T, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = z[k] ? -1e9f : T[k];
-    } break;
-    case 23: {  // LOOSE_INV: 1 / protected(T)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = loose_denom(T[k]);
-    }
-      SR_CALL1(v_rcp)
-    case 24: SR_EACH(T[k] = fabsf(T[k]))
-    case 25: SR_EACH(T[k] = -T[k])
-    case 26: SR_CALL1(v_sqrt)
-    case 27: {
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = fabsf(T[k]);
-    }
-      SR_CALL1(v_sqrt)
-    case 32: {  // exp clamped at 80 (extension)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = fminf(T[k], 80.0f);
-    }
-      SR_CALL1(v_exp)
-    default: SR_EACH(T[k] = 0.0f)
-  }
-}
-
-#undef SR_EACH
-#undef SR_CALL1
-#undef SR_CALL2
-
-// Run one compiled program over the warp's DPT x 32 datapoints of a tile.
-// xs points at the tile's first datapoint of X row 0; rows are xrs floats
-// apart.
-template <int DPT>
-__device__ __forceinline__ void run_program(const Instr *__restrict__ code,
-                                            int len, const float *xs, int xrs,
-                                            const SpillStack &st, int lane,
-                                            const float *cache, int64_t ldc, int64_t dp0,
-                                            float (&T)[DPT]) {
-  // Every program starts with an instruction that loads T.
-  uint4 ins = ldg_instr(code);
-  for (int i = 0; i < len; ++i) {
-    // The code buffer ends with a padding instruction, so this prefetch of
-    // the next word is always in bounds.
-    const uint4 nxt = ldg_instr(code + i + 1);
-    const uint32_t w = ins.x;
-    if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
-    if (instr_load(w))
-      load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
-    float b[DPT];
-    const uint32_t bk = instr_b_kind(w);
-    if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, xrs, st, lane, cache, ldc, dp0);
-    apply_op<DPT>(instr_op(w), T, b);
-    ins = nxt;
-  }
-}
 
 // MAXW / MINB: launch bounds of the instantiation (at most MAXW evaluating
 // warps, at least MINB resident blocks per SM), which set the register budget.
@@ -508,43 +68,10 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
   const int n_items = p.n_groups * p.n_spans;
 
   if (warp == W) {
-    // ---------------- producer: one thread ----------------
-    if (lane != 0) return;
-    uint32_t buf = 0, phase = 0;
-    uint32_t armed = 0;  // buffers with a copy in flight
-    uint32_t armed_parity0 = 0, armed_parity1 = 0;
-    const uint32_t row_bytes = static_cast<uint32_t>(span) * sizeof(float);
-    for (;;) {
-      const int item = atomicAdd(p.work_counter, 1);
-      if (!mbar_wait(&empty[buf], phase ^ 1u, p.error)) {
-        // Let copies already issued land before the block exits.
-        if (armed & 1u) mbar_drain(&full[0], armed_parity0);
-        if (armed & 2u) mbar_drain(&full[1], armed_parity1);
-        return;
-      }
-      // The consumers released this buffer, so its previous copy landed.
-      armed &= ~(1u << buf);
-      if (item >= n_items) {
-        desc[buf] = ItemDesc{-1, 0, 0, 0};
-        mbar_arrive(&full[buf]);
-        return;
-      }
-      const int group = item % p.n_groups;
-      const int sp = item / p.n_groups;
-      desc[buf] = ItemDesc{item, group, sp, 0};
-      mbar_arrive_expect_tx(&full[buf], row_bytes * rows);
-      const float *src = p.X + static_cast<int64_t>(sp) * span;
-      float *dst = xbuf + static_cast<size_t>(buf) * rows * span;
-      for (int v = 0; v < rows; ++v)
-        bulk_g2s(dst + static_cast<size_t>(v) * span, src + v * p.ldx, row_bytes, &full[buf]);
-      armed |= 1u << buf;
-      if (buf == 0) armed_parity0 = phase;
-      else armed_parity1 = phase;
-      if (++buf == kBufs) {
-        buf = 0;
-        phase ^= 1u;
-      }
-    }
+    if (lane == 0)
+      run_producer(p.n_groups, n_items, p.work_counter, p.error, p.X, p.ldx, rows, span, xbuf,
+                   desc, full, empty);
+    return;
   }
 
   // ---------------- evaluating warps ----------------
@@ -807,6 +334,12 @@ cudaError_t launch_interp(int dpt, bool pred, const EvalArgs &args, int blocks,
                           size_t smem, cudaStream_t stream) {
   const void *fn = select_interp(dpt, pred, args.W);
   if (!fn || args.W < 1 || args.W > kMaxWarps) return cudaErrorInvalidValue;
+  // Plans of one instantiation can differ in shared-memory size (main and
+  // cache-fill sets, autotune candidates); the attribute belongs to the
+  // kernel, so set it for this launch.
+  const cudaError_t err = cudaFuncSetAttribute(
+      fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
   void *params[] = {const_cast<EvalArgs *>(&args)};
   return cudaLaunchKernel(fn, dim3(blocks), dim3((args.W + 1) * 32), params, smem, stream);
 }

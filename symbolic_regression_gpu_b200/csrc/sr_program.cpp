@@ -136,8 +136,10 @@ inline uint32_t reversed(int tok) {
 struct Emitter {
   const std::vector<Node> &nodes;
   std::vector<Instr> &out;
+  size_t first = 0;          // index of this program's first instruction in `out`
   int pending_spill = -1;
   int sp = 0;
+  int spill_at[kMaxSpillSlots + 1] = {};  // instruction that spilled into each slot
 
   // [spill] [T = load] [b = operand] T = op(T, b)
   void emit(uint32_t op, const Node *load, uint32_t bk, uint32_t bp, uint32_t bc) {
@@ -150,12 +152,16 @@ struct Emitter {
       ins.a = load->lp;
       ac = load->lconst;
     }
+    const int index = static_cast<int>(out.size() - first);
     if (pending_spill >= 0) {
       ins.w |= kSpillBit | (static_cast<uint32_t>(pending_spill) << 13);
+      spill_at[pending_spill] = index;
       pending_spill = -1;
     }
     ins.b = bp;
-    ins.c = (ac & 0x3FFu) | ((bc & 0x3FFu) << 10);
+    // A spilled operand is the accumulator value right before its spill.
+    const uint32_t producer = (bk == kBS) ? static_cast<uint32_t>(spill_at[bp] - 1) : 0u;
+    ins.c = (ac & 0x3FFu) | ((bc & 0x3FFu) << 10) | ((producer & 0x3FFu) << 20);
     out.push_back(ins);
   }
 
@@ -367,7 +373,7 @@ sr_status compile_expression(const int32_t *tok, const double *val, int len,
   }
 
   const size_t first = out.size();
-  Emitter em{nodes, out};
+  Emitter em{nodes, out, first};
   em.gen(root);
   info.n_instr = static_cast<int32_t>(out.size() - first);
 

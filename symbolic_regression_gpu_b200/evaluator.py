@@ -166,7 +166,7 @@ class Evaluator:
                                                  dp_count, _f32ptr(out)), "sr_eval_predictions")
         return out
 
-    def eval_grad(self, pop: Population, mode: int = _lib.SR_GRAD_RECOMPUTE):
+    def eval_grad(self, pop: Population, mode: int = _lib.SR_GRAD_CHECKPOINT):
         """(mse [E], d mse / d constants [C]) with constants in token order."""
         nconst = int(np.count_nonzero(pop.tokens == 0))
         mse = np.empty(pop.num_exprs, np.float32)
@@ -179,7 +179,7 @@ class Evaluator:
 
     def optimize_constants(self, pop: Population, steps: int = 20, lr: float = 0.05,
                            beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8,
-                           mode: int = _lib.SR_GRAD_RECOMPUTE):
+                           mode: int = _lib.SR_GRAD_CHECKPOINT):
         """On-device Adam over every expression's constants.
         Returns (constants [C] after `steps`, mse [E] at those constants)."""
         nconst = int(np.count_nonzero(pop.tokens == 0))

@@ -111,3 +111,170 @@ def run_bytecode(code, X, V, n_slots=16):
             assert 1 <= op <= 9 or 41 <= op <= 49, f"unary opcode {op} with operand"
             T = _bin(op, T, vb)
     return T
+
+
+# ---- FP64 reverse mode over the compiled bytecode ---------------------------
+
+def _op64(op, a, b):
+    """Operator semantics in float64 (the FP64 oracle's sro_op_f64)."""
+    with np.errstate(all="ignore"):
+        if op == 0:
+            return a
+        if op in (8, 23):
+            d = b if op == 8 else a
+            eps = np.full_like(d, 1e-9)  # the operand's dtype
+            d = np.where(np.abs(d) <= eps, np.where(d < 0, -eps, eps), d)
+            return a / d if op == 8 else 1.0 / d
+        f = {1: lambda: a + b, 2: lambda: a - b, 3: lambda: a * b,
+             4: lambda: np.where(b == 0, np.nan, a / np.where(b == 0, 1.0, b)),
+             5: lambda: np.power(a, b), 6: lambda: np.fmin(a, b), 7: lambda: np.fmax(a, b),
+             9: lambda: np.where((a == 0) & (b == 0), 0.0, np.power(np.abs(a), b)),
+             10: lambda: np.sin(a), 11: lambda: np.cos(a), 12: lambda: np.tan(a),
+             13: lambda: np.sinh(a), 14: lambda: np.cosh(a), 15: lambda: np.tanh(a),
+             16: lambda: np.exp(a), 17: lambda: np.log(a), 18: lambda: 1.0 / a,
+             19: lambda: np.arcsin(a), 20: lambda: np.arccos(a), 21: lambda: np.arctan(a),
+             22: lambda: np.where(a == 0, -1e9, np.log(np.abs(a))), 24: lambda: np.abs(a),
+             25: lambda: -a, 26: lambda: np.sqrt(a), 27: lambda: np.sqrt(np.abs(a)),
+             32: lambda: np.exp(np.fmin(a, 80.0))}[op]
+        return f()
+
+
+def _partials64(op, a, b, out):
+    """(d out / d a, d out / d b) with the conventions of the device adjoint."""
+    one, zero = np.ones_like(a), np.zeros_like(a)
+    sg = np.sign
+    with np.errstate(all="ignore"):
+        if op == 0:
+            return one, zero
+        if op == 1:
+            return one, one
+        if op == 2:
+            return one, -one
+        if op == 3:
+            return b, a
+        if op == 4:  # the device forms 1/b once and reuses it
+            r = 1.0 / b
+            return r, -out * r
+        if op == 5:
+            return b * np.power(a, b - 1.0), out * np.log(a)
+        if op in (6, 7):
+            first = np.isnan(b) | (~np.isnan(a) & ((a <= b) if op == 6 else (a >= b)))
+            return first.astype(np.float64), (~first).astype(np.float64)
+        if op == 8:
+            tiny = np.abs(b) <= 1e-9
+            eps = np.full_like(b, 1e-9)  # the operand's dtype
+            r = 1.0 / np.where(tiny, np.where(b < 0, -eps, eps), b)
+            return r, np.where(tiny, 0.0, -out * r)
+        if op == 9:
+            z = (a == 0) & (b == 0)
+            return (np.where(z, 0.0, b * np.power(np.abs(a), b - 1.0) * sg(a)),
+                    np.where(z, 0.0, out * np.log(np.abs(a))))
+        d = {10: lambda: np.cos(a), 11: lambda: -np.sin(a), 12: lambda: 1.0 + out * out,
+             13: lambda: np.cosh(a), 14: lambda: np.sinh(a), 15: lambda: 1.0 - out * out,
+             16: lambda: out, 17: lambda: 1.0 / a, 18: lambda: -out * out,
+             19: lambda: 1.0 / np.sqrt(1.0 - a * a), 20: lambda: -1.0 / np.sqrt(1.0 - a * a),
+             21: lambda: 1.0 / (1.0 + a * a), 22: lambda: np.where(a == 0, 0.0, 1.0 / a),
+             23: lambda: np.where(np.abs(a) <= 1e-9, 0.0, -out * out), 24: lambda: sg(a),
+             25: lambda: -one, 26: lambda: 0.5 / out,
+             27: lambda: np.where(a == 0, 0.0, sg(a) * 0.5 / out),
+             32: lambda: np.where(a < 80.0, out, 0.0)}[op]()
+        return d, zero
+
+
+def _strong(g, d):
+    with np.errstate(all="ignore"):
+        return np.where(g == 0, 0.0, g * d)
+
+
+def adjoint_bytecode(code, X, V, n_const, n_slots=16, dtype=np.float64, with_abs=False):
+    """MSE and d MSE / d constants of one compiled program, run the way the
+    adjoint kernel runs it: a forward pass recording every instruction's
+    output (the tape), then a backward pass in reverse instruction order with
+    an adjoint accumulator and adjoint spill slots.  A spilled operand's value
+    is read back from the tape at the producer index held in bits 20-29 of the
+    instruction's c word; the forward pass asserts that it equals the value
+    the spill slot holds.  Constants enter as their float32 bits widened.
+    dtype=np.float64: the FP64 restatement.  dtype=np.float32: every value,
+    partial and adjoint product rounded to float32 (the device's arithmetic,
+    numpy's libm), constant gradients accumulated in float64.  with_abs adds
+    the mean over valid datapoints of |adjoint reaching each constant|."""
+    N = X.shape[1]
+    D = dtype
+    y = X[V].astype(D)
+    S = [np.zeros(N, D) for _ in range(n_slots)]
+    tape = []
+    T = np.zeros(N, D)
+
+    def leaf(kind, payload):
+        if kind == 0:
+            return X[int(payload)].astype(D)
+        return np.full(N, D(np.array([payload], np.uint32).view(F)[0]))
+
+    def operand(bk, payload):
+        return {2: lambda: X[int(payload)].astype(D),
+                3: lambda: np.full(N, D(np.array([payload], np.uint32).view(F)[0]))}[bk]()
+
+    for i, (w, a, b, c) in enumerate(code):
+        w, c = int(w), int(c)
+        op, bk = w & 63, (w >> 9) & 7
+        if w & (1 << 12):
+            S[(w >> 13) & 31] = T.copy()
+        if w & (1 << 6):
+            T = leaf((w >> 7) & 3, a)
+        if bk == 0:
+            T = _op64(op, T, None)
+        else:
+            if bk == 1:
+                vb = S[int(b)]
+                prod = (c >> 20) & 0x3FF
+                assert prod < i and np.array_equal(vb, tape[prod], equal_nan=True), \
+                    f"instruction {i}: spilled operand is not the output of instruction {prod}"
+            else:
+                vb = operand(bk, b)
+            T = _op64(op - 40, vb, T) if op > 40 else _op64(op, T, vb)
+        T = np.asarray(T, D)
+        tape.append(T.copy())
+    with np.errstate(all="ignore"):
+        valid = ~np.isnan(T) & ~np.isinf(T.astype(np.float32))
+    cnt = int(valid.sum())
+    d = np.where(valid, T - y, 0.0).astype(D)
+    mse = (d.astype(np.float64) ** 2).sum() / cnt if cnt else np.nan
+    grad = np.zeros(n_const, np.float64)
+    gabs = np.zeros(n_const, np.float64)
+    gT = (2.0 * d).astype(D)
+    G = [np.zeros(N, D) for _ in range(n_slots)]
+    for i in range(len(code) - 1, -1, -1):
+        w, a, b, c = (int(q) for q in code[i])
+        op, bk = w & 63, (w >> 9) & 7
+        to = tape[i]
+        ti = leaf((w >> 7) & 3, a) if w & (1 << 6) else tape[i - 1]
+        if bk == 1:
+            bv = tape[(c >> 20) & 0x3FF]
+        elif bk:
+            bv = operand(bk, b)
+        else:
+            bv = np.zeros(N, D)
+        if bk == 0:
+            dT, db = _partials64(op, ti, None, to)
+        elif op > 40:
+            db, dT = _partials64(op - 40, bv, ti, to)
+        else:
+            dT, db = _partials64(op, ti, bv, to)
+        gi = _strong(gT, np.asarray(dT, D)).astype(D)
+        gb = _strong(gT, np.asarray(db, D)).astype(D)
+        if bk == 3:
+            grad[(c >> 10) & 0x3FF] += gb.sum(dtype=np.float64)
+            gabs[(c >> 10) & 0x3FF] += np.abs(gb).sum(dtype=np.float64)
+        elif bk == 1:
+            G[b] = gb
+        if w & (1 << 6):
+            if (w >> 7) & 3 == 1:
+                grad[c & 0x3FF] += gi.sum(dtype=np.float64)
+                gabs[c & 0x3FF] += np.abs(gi).sum(dtype=np.float64)
+            gT = G[(w >> 13) & 31] if w & (1 << 12) else np.zeros(N, D)
+        else:
+            gT = gi
+    g = grad / cnt if cnt else np.full(n_const, np.nan)
+    if with_abs:
+        return mse, g, (gabs / cnt if cnt else np.full(n_const, np.nan))
+    return mse, g
