@@ -2,20 +2,26 @@
 // every expression's constants, and on-device Adam over those constants.
 // (No reference counterpart: the reference evaluates MSE only.)
 //
-//   adj_kernel<DPT=4>       fused forward + backward per tile.  Same work
-//                           decomposition as interp_kernel (producer thread
-//                           streaming X spans into shared memory, warps claiming
-//                           expressions of a group).  Per tile a warp
-//                           (1) runs the program forward, writing every
-//                           instruction's output into its shared-memory tape;
-//                           (2) forms the squared-error epilogue and the seed
+//   adj_kernel<GTAPE>       fused forward + backward per tile.  Same work
+//                           decomposition as interp_kernel (a producer thread
+//                           streaming X spans into shared memory, warps
+//                           claiming expressions of a group).  Per tile a warp
+//                           (1) runs the program forward; each instruction's
+//                           dispatch computes its value and its local partials
+//                           (d out / d T, and d out / d b when b is a constant
+//                           or a spilled subtree), and the partials go to the
+//                           warp's Jacobian tape;
+//                           (2) forms the squared error and the seed
 //                           2 (pred - y) for valid datapoints (0 otherwise);
-//                           (3) replays the program backwards: an adjoint
-//                           accumulator gT and adjoint spill slots mirror the
-//                           forward ones, each instruction's local partials
-//                           come from its tape values, constant leaves
-//                           accumulate gT * partial into per-lane FP64
-//                           accumulators.  At the end of a span the
+//                           (3) sweeps the tape backwards: an adjoint
+//                           accumulator gT, adjoint spill slots mirroring the
+//                           forward ones, and per-lane FP64 accumulators for
+//                           the constants.  The sweep has no operator code at
+//                           all and stops at the lowest instruction that holds
+//                           a constant.
+//                           The tape lives in shared memory, or per warp in
+//                           global scratch (GTAPE) for programs whose tape
+//                           does not fit.  At the end of a span the constant
 //                           accumulators are reduced over the warp and added
 //                           to grad_acc (FP64 atomics).
 //   grad_finalize_kernel    mse = sum / count per expression and
@@ -30,7 +36,9 @@
 // operand they return (the first on ties, the non-NaN one if one is NaN);
 // 0^0 of LOOSE_POW has derivative 0.  A zero adjoint times an infinite or NaN
 // partial is zero ("strong zero"), so datapoints and branches that do not
-// reach the result contribute exactly nothing.
+// reach the result contribute exactly nothing.  Values are computed exactly as
+// the forward interpreter computes them (same routines, same rounding), so the
+// MSE of a gradient call equals the forward MSE up to summation order.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,214 +48,305 @@
 namespace sr {
 namespace {
 
-constexpr int kAdjDpt = 4;
+#ifndef SR_ADJ_DPT
+#define SR_ADJ_DPT 4
+#endif
+constexpr int kAdjDpt = SR_ADJ_DPT;  // datapoints per thread (4 or 8)
+static_assert(kAdjDpt == 4 || kAdjDpt == 8, "adjoint DPT 4 or 8");
 
 __device__ __forceinline__ float strong_mul(float g, float d) { return g == 0.0f ? 0.0f : g * d; }
 
 __device__ __forceinline__ float signf(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
 
-// Partials of f(u, v) for binary token `tok` (u first / left operand);
-// `out` is f(u, v).  Transcendental pieces go through the out-of-line
-// 4-wide routines.
-template <int DPT>
-__device__ __forceinline__ void binary_partials(int tok, const float (&u)[DPT],
-                                                const float (&v)[DPT], const float (&out)[DPT],
-                                                float (&du)[DPT], float (&dv)[DPT]) {
-  switch (tok) {
-    case 1:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { du[k] = 1.0f; dv[k] = 1.0f; }
-      break;
-    case 2:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { du[k] = 1.0f; dv[k] = -1.0f; }
-      break;
-    case 3:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { du[k] = v[k]; dv[k] = u[k]; }
-      break;
-    case 4: {  // u / v
-      float r[DPT];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(r, h, v_rcp(quad<DPT>(v, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { du[k] = r[k]; dv[k] = -out[k] * r[k]; }
-    } break;
-    case 5: {  // u^v: du = v u^(v-1), dv = u^v ln u
-      float vm1[DPT], pw[DPT], lg[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) vm1[k] = v[k] - 1.0f;
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) {
-        unquad<DPT>(pw, h, v_pow(quad<DPT>(u, h), quad<DPT>(vm1, h)));
-        unquad<DPT>(lg, h, v_log(quad<DPT>(u, h)));
-      }
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { du[k] = v[k] * pw[k]; dv[k] = out[k] * lg[k]; }
-    } break;
-    case 6:  // fminf(u, v)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        const bool first = isnan(v[k]) || (!isnan(u[k]) && u[k] <= v[k]);
-        du[k] = first ? 1.0f : 0.0f;
-        dv[k] = first ? 0.0f : 1.0f;
-      }
-      break;
-    case 7:  // fmaxf(u, v)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        const bool first = isnan(v[k]) || (!isnan(u[k]) && u[k] >= v[k]);
-        du[k] = first ? 1.0f : 0.0f;
-        dv[k] = first ? 0.0f : 1.0f;
-      }
-      break;
-    case 8: {  // u / protected(v)
-      float d[DPT], r[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) d[k] = loose_denom(v[k]);
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(r, h, v_rcp(quad<DPT>(d, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        du[k] = r[k];
-        dv[k] = (fabsf(v[k]) <= 1e-9f) ? 0.0f : -out[k] * r[k];
-      }
-    } break;
-    case 9: {  // (u == 0 && v == 0) ? 0 : |u|^v
-      float a[DPT], vm1[DPT], pw[DPT], lg[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { a[k] = fabsf(u[k]); vm1[k] = v[k] - 1.0f; }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) {
-        unquad<DPT>(pw, h, v_pow(quad<DPT>(a, h), quad<DPT>(vm1, h)));
-        unquad<DPT>(lg, h, v_log(quad<DPT>(a, h)));
-      }
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        const bool z = (u[k] == 0.0f && v[k] == 0.0f);
-        du[k] = z ? 0.0f : v[k] * pw[k] * signf(u[k]);
-        dv[k] = z ? 0.0f : out[k] * lg[k];
-      }
-    } break;
-    default:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) { du[k] = 0.0f; dv[k] = 0.0f; }
-      break;
+// ---- value + derivative routines, out of line ------------------------------
+// Each routine exists once per width SR_ADJ_WIDTH (datapoints per call: 1, 2
+// or 4).  Narrow routines keep the hot code small (instruction cache); wide
+// ones give the scheduler independent work inside one call.
+#ifndef SR_ADJ_WIDTH
+#define SR_ADJ_WIDTH 1
+#endif
+static_assert(SR_ADJ_WIDTH == 1 || SR_ADJ_WIDTH == 2 || SR_ADJ_WIDTH == 4, "width 1, 2 or 4");
+
+struct VD1 {
+  float v, d;
+};
+struct VD2 {
+  float v, du, dv;
+};
+struct VD4 {
+  float4 v, d;
+};
+
+#define SR_VD1(NAME, VAL, DER)                                       \
+  __device__ __forceinline__ VD1 NAME##_body(float x) {              \
+    const float o = (VAL);                                           \
+    return VD1{o, (DER)};                                            \
+  }                                                                  \
+  __device__ __noinline__ VD1 NAME##_w1(float x) { return NAME##_body(x); } \
+  __device__ __noinline__ float4 NAME##_w2(float x0, float x1) {     \
+    const VD1 a = NAME##_body(x0), b = NAME##_body(x1);              \
+    return make_float4(a.v, a.d, b.v, b.d);                          \
+  }                                                                  \
+  __device__ __noinline__ VD4 NAME##_w4(float4 x) {                 \
+    const VD1 a = NAME##_body(x.x), b = NAME##_body(x.y);            \
+    const VD1 c = NAME##_body(x.z), e = NAME##_body(x.w);            \
+    return VD4{make_float4(a.v, b.v, c.v, e.v), make_float4(a.d, b.d, c.d, e.d)}; \
   }
+SR_VD1(g_sin, sinf(x), cosf(x))
+SR_VD1(g_cos, cosf(x), -sinf(x))
+SR_VD1(g_tan, tanf(x), __fadd_rn(1.0f, __fmul_rn(o, o)))
+SR_VD1(g_sinh, sinhf(x), coshf(x))
+SR_VD1(g_cosh, coshf(x), sinhf(x))
+SR_VD1(g_tanh, tanhf(x), __fsub_rn(1.0f, __fmul_rn(o, o)))
+SR_VD1(g_exp, expf(x), o)
+SR_VD1(g_log, logf(x), __frcp_rn(x))
+SR_VD1(g_rcp, __frcp_rn(x), __fmul_rn(-o, o))
+SR_VD1(g_asin, asinf(x), __frcp_rn(__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(x, x)))))
+SR_VD1(g_acos, acosf(x), -__frcp_rn(__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(x, x)))))
+SR_VD1(g_atan, atanf(x), __frcp_rn(__fadd_rn(1.0f, __fmul_rn(x, x))))
+SR_VD1(g_llog, (x == 0.0f) ? -1e9f : logf(fabsf(x)), (x == 0.0f) ? 0.0f : __frcp_rn(x))
+SR_VD1(g_linv, __frcp_rn(loose_denom(x)), (fabsf(x) <= 1e-9f) ? 0.0f : __fmul_rn(-o, o))
+SR_VD1(g_sqrt, __fsqrt_rn(x), __frcp_rn(2.0f * o))
+SR_VD1(g_lsqrt, __fsqrt_rn(fabsf(x)), (x == 0.0f) ? 0.0f : signf(x) * __frcp_rn(2.0f * o))
+SR_VD1(g_expc, expf(fminf(x, 80.0f)), (x < 80.0f) ? o : 0.0f)
+#undef SR_VD1
+
+// u^v: du = v u^(v-1), dv = u^v ln u.
+__device__ __forceinline__ VD2 g_pow_body(float u, float v) {
+  const float o = powf(u, v);
+  return VD2{o, __fmul_rn(v, powf(u, __fsub_rn(v, 1.0f))), __fmul_rn(o, logf(u))};
+}
+// LOOSE_POW u, v: 0^0 = 0, else |u|^v; du = v |u|^(v-1) sign(u), dv = out ln|u|.
+__device__ __forceinline__ VD2 g_lpow_body(float u, float v) {
+  const bool z = (u == 0.0f && v == 0.0f);
+  const float a = fabsf(u);
+  const float o = z ? 0.0f : powf(a, v);
+  return VD2{o, z ? 0.0f : __fmul_rn(__fmul_rn(v, powf(a, __fsub_rn(v, 1.0f))), signf(u)),
+             z ? 0.0f : __fmul_rn(o, logf(a))};
+}
+// Division u / d with 1/d reused for both partials: du = 1/d, dv = -out/d
+// (0 where `flat`, the protected region of LOOSE_DIV); NaN at d == 0 when
+// nan_at_zero (DIV).
+__device__ __forceinline__ VD2 g_div_body(float u, float d, bool flat, bool nan_at_zero) {
+  const float q = __fdiv_rn(u, d);
+  const float o = (nan_at_zero && d == 0.0f) ? qnan() : q;
+  const float rc = __frcp_rn(d);
+  return VD2{o, rc, flat ? 0.0f : __fmul_rn(-o, rc)};
+}
+__device__ __noinline__ VD2 g_pow_w1(float u, float v) { return g_pow_body(u, v); }
+__device__ __noinline__ VD2 g_lpow_w1(float u, float v) { return g_lpow_body(u, v); }
+__device__ __noinline__ VD2 g_div_w1(float u, float d, bool flat, bool nz) {
+  return g_div_body(u, d, flat, nz);
+}
+template <int N>
+struct VD2N {
+  float v[N], du[N], dv[N];
+};
+__device__ __noinline__ VD2N<2> g_pow_w2(float u0, float u1, float v0, float v1) {
+  const VD2 a = g_pow_body(u0, v0), b = g_pow_body(u1, v1);
+  return VD2N<2>{{a.v, b.v}, {a.du, b.du}, {a.dv, b.dv}};
+}
+__device__ __noinline__ VD2N<2> g_lpow_w2(float u0, float u1, float v0, float v1) {
+  const VD2 a = g_lpow_body(u0, v0), b = g_lpow_body(u1, v1);
+  return VD2N<2>{{a.v, b.v}, {a.du, b.du}, {a.dv, b.dv}};
+}
+__device__ __noinline__ VD2N<2> g_div_w2(float u0, float u1, float d0, float d1, bool f0, bool f1,
+                                         bool nz) {
+  const VD2 a = g_div_body(u0, d0, f0, nz), b = g_div_body(u1, d1, f1, nz);
+  return VD2N<2>{{a.v, b.v}, {a.du, b.du}, {a.dv, b.dv}};
+}
+__device__ __noinline__ VD2N<4> g_pow_w4(float4 u, float4 v) {
+  const VD2 a = g_pow_body(u.x, v.x), b = g_pow_body(u.y, v.y);
+  const VD2 c = g_pow_body(u.z, v.z), e = g_pow_body(u.w, v.w);
+  return VD2N<4>{{a.v, b.v, c.v, e.v}, {a.du, b.du, c.du, e.du}, {a.dv, b.dv, c.dv, e.dv}};
+}
+__device__ __noinline__ VD2N<4> g_lpow_w4(float4 u, float4 v) {
+  const VD2 a = g_lpow_body(u.x, v.x), b = g_lpow_body(u.y, v.y);
+  const VD2 c = g_lpow_body(u.z, v.z), e = g_lpow_body(u.w, v.w);
+  return VD2N<4>{{a.v, b.v, c.v, e.v}, {a.du, b.du, c.du, e.du}, {a.dv, b.dv, c.dv, e.dv}};
+}
+__device__ __noinline__ VD2N<4> g_div_w4(float4 u, float4 d, uint32_t flat, bool nz) {
+  const VD2 a = g_div_body(u.x, d.x, flat & 1u, nz), b = g_div_body(u.y, d.y, flat & 2u, nz);
+  const VD2 c = g_div_body(u.z, d.z, flat & 4u, nz), e = g_div_body(u.w, d.w, flat & 8u, nz);
+  return VD2N<4>{{a.v, b.v, c.v, e.v}, {a.du, b.du, c.du, e.du}, {a.dv, b.dv, c.dv, e.dv}};
 }
 
-// Derivative of unary token `tok` at x, with out = f(x).
+// T, dT = f(T), f'(T) for DPT datapoints through the routine of width SR_ADJ_WIDTH.
+#if SR_ADJ_WIDTH == 1
+#define SR_G1(FN)                                                          \
+  {                                                                        \
+    _Pragma("unroll") for (int k = 0; k < DPT; ++k) {                      \
+      const VD1 r = FN##_w1(T[k]);                                         \
+      T[k] = r.v;                                                          \
+      dT[k] = r.d;                                                         \
+    }                                                                      \
+  }                                                                        \
+  break;
+#elif SR_ADJ_WIDTH == 2
+#define SR_G1(FN)                                                          \
+  {                                                                        \
+    _Pragma("unroll") for (int k = 0; k < DPT; k += 2) {                   \
+      const float4 r = FN##_w2(T[k], T[k + 1]);                            \
+      T[k] = r.x;                                                          \
+      dT[k] = r.y;                                                         \
+      T[k + 1] = r.z;                                                      \
+      dT[k + 1] = r.w;                                                     \
+    }                                                                      \
+  }                                                                        \
+  break;
+#else
+#define SR_G1(FN)                                                          \
+  {                                                                        \
+    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h) {                  \
+      const VD4 r = FN##_w4(quad<DPT>(T, h));                              \
+      unquad<DPT>(T, h, r.v);                                              \
+      unquad<DPT>(dT, h, r.d);                                             \
+    }                                                                      \
+  }                                                                        \
+  break;
+#endif
+
+// (out, d/dleft, d/dright) of a binary routine for all DPT datapoints.
 template <int DPT>
-__device__ __forceinline__ void unary_partial(int tok, const float (&x)[DPT],
-                                              const float (&out)[DPT], float (&dx)[DPT]) {
-  switch (tok) {
-    case 0:
+__device__ __forceinline__ void binary_vd(int which, const float (&u)[DPT], const float (&v)[DPT],
+                                          const bool (&flat)[DPT], bool nz, float (&o)[DPT],
+                                          float (&du)[DPT], float (&dv)[DPT]) {
+#if SR_ADJ_WIDTH == 1
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = 1.0f;
-      break;
-    case 10:
+  for (int k = 0; k < DPT; ++k) {
+    const VD2 r = which == 0 ? g_pow_w1(u[k], v[k])
+                             : (which == 1 ? g_lpow_w1(u[k], v[k]) : g_div_w1(u[k], v[k], flat[k], nz));
+    o[k] = r.v;
+    du[k] = r.du;
+    dv[k] = r.dv;
+  }
+#elif SR_ADJ_WIDTH == 2
 #pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_cos(quad<DPT>(x, h)));
-      break;
-    case 11:
+  for (int k = 0; k < DPT; k += 2) {
+    const VD2N<2> r = which == 0 ? g_pow_w2(u[k], u[k + 1], v[k], v[k + 1])
+                      : which == 1 ? g_lpow_w2(u[k], u[k + 1], v[k], v[k + 1])
+                                   : g_div_w2(u[k], u[k + 1], v[k], v[k + 1], flat[k], flat[k + 1], nz);
 #pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_sin(quad<DPT>(x, h)));
+    for (int q = 0; q < 2; ++q) {
+      o[k + q] = r.v[q];
+      du[k + q] = r.du[q];
+      dv[k + q] = r.dv[q];
+    }
+  }
+#else
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = -dx[k];
-      break;
-    case 12:
+  for (int h = 0; h < DPT / 4; ++h) {
+    uint32_t fl = 0;
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = 1.0f + out[k] * out[k];
-      break;
-    case 13:
+    for (int q = 0; q < 4; ++q) fl |= flat[4 * h + q] ? (1u << q) : 0u;
+    const VD2N<4> r = which == 0 ? g_pow_w4(quad<DPT>(u, h), quad<DPT>(v, h))
+                      : which == 1 ? g_lpow_w4(quad<DPT>(u, h), quad<DPT>(v, h))
+                                   : g_div_w4(quad<DPT>(u, h), quad<DPT>(v, h), fl, nz);
 #pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_cosh(quad<DPT>(x, h)));
-      break;
-    case 14:
+    for (int q = 0; q < 4; ++q) {
+      o[4 * h + q] = r.v[q];
+      du[4 * h + q] = r.du[q];
+      dv[4 * h + q] = r.dv[q];
+    }
+  }
+#endif
+}
+
+// T = op(T, b) exactly as apply_op computes it, plus dT = d out / d T and
+// db = d out / d b (left unset for unary operators).
+#define SR_EACH2(STMT)                                           \
+  {                                                              \
+    _Pragma("unroll") for (int k = 0; k < DPT; ++k) { STMT; }   \
+  }                                                              \
+  break;
+// Binary routine `which` (0 pow, 1 loose pow, 2 division) on (left, right);
+// REV: T is the right operand.
+#define SR_G2(WHICH, REV, NZ)                                              \
+  {                                                                        \
+    float o_[DPT], dl_[DPT], dr_[DPT];                                     \
+    if (REV)                                                               \
+      binary_vd<DPT>(WHICH, b, T, flat, NZ, o_, dl_, dr_);                 \
+    else                                                                   \
+      binary_vd<DPT>(WHICH, T, b, flat, NZ, o_, dl_, dr_);                 \
+    _Pragma("unroll") for (int k = 0; k < DPT; ++k) {                      \
+      T[k] = o_[k];                                                        \
+      dT[k] = REV ? dr_[k] : dl_[k];                                       \
+      db[k] = REV ? dl_[k] : dr_[k];                                       \
+    }                                                                      \
+  }                                                                        \
+  break;
+
+template <int DPT>
+__device__ __forceinline__ void apply_op_grad(uint32_t op, float (&T)[DPT], float (&b)[DPT],
+                                              float (&dT)[DPT], float (&db)[DPT]) {
+  bool flat[DPT];
 #pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_sinh(quad<DPT>(x, h)));
-      break;
-    case 15:
+  for (int k = 0; k < DPT; ++k) flat[k] = false;
+  switch (op) {
+    case 0: SR_EACH2(dT[k] = 1.0f)
+    case 1: SR_EACH2(T[k] = __fadd_rn(T[k], b[k]); dT[k] = 1.0f; db[k] = 1.0f)
+    case 2: SR_EACH2(T[k] = __fsub_rn(T[k], b[k]); dT[k] = 1.0f; db[k] = -1.0f)
+    case 42: SR_EACH2(T[k] = __fsub_rn(b[k], T[k]); dT[k] = -1.0f; db[k] = 1.0f)
+    case 3: SR_EACH2(db[k] = T[k]; dT[k] = b[k]; T[k] = __fmul_rn(T[k], b[k]))
+    case 4: SR_G2(2, false, true)
+    case 44: SR_G2(2, true, true)
+    case 5: SR_G2(0, false, false)
+    case 45: SR_G2(0, true, false)
+    case 6:
+      SR_EACH2(const bool f = isnan(b[k]) || (!isnan(T[k]) && T[k] <= b[k]);
+               T[k] = fminf(T[k], b[k]); dT[k] = f ? 1.0f : 0.0f; db[k] = f ? 0.0f : 1.0f)
+    case 46:
+      SR_EACH2(const bool f = isnan(T[k]) || (!isnan(b[k]) && b[k] <= T[k]);
+               T[k] = fminf(b[k], T[k]); db[k] = f ? 1.0f : 0.0f; dT[k] = f ? 0.0f : 1.0f)
+    case 7:
+      SR_EACH2(const bool f = isnan(b[k]) || (!isnan(T[k]) && T[k] >= b[k]);
+               T[k] = fmaxf(T[k], b[k]); dT[k] = f ? 1.0f : 0.0f; db[k] = f ? 0.0f : 1.0f)
+    case 47:
+      SR_EACH2(const bool f = isnan(T[k]) || (!isnan(b[k]) && b[k] >= T[k]);
+               T[k] = fmaxf(b[k], T[k]); db[k] = f ? 1.0f : 0.0f; dT[k] = f ? 0.0f : 1.0f)
+    case 8: {  // T / protected(b)
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = 1.0f - out[k] * out[k];
-      break;
-    case 16:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = out[k];
-      break;
-    case 17:
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_rcp(quad<DPT>(x, h)));
-      break;
-    case 18:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = -out[k] * out[k];
-      break;
-    case 19:
-    case 20: {
-      float t[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) t[k] = 1.0f - x[k] * x[k];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(t, h, v_sqrt(quad<DPT>(t, h)));
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_rcp(quad<DPT>(t, h)));
-      if (tok == 20) {
-#pragma unroll
-        for (int k = 0; k < DPT; ++k) dx[k] = -dx[k];
+      for (int k = 0; k < DPT; ++k) {
+        flat[k] = fabsf(b[k]) <= 1e-9f;
+        b[k] = loose_denom(b[k]);
       }
-    } break;
-    case 21: {
-      float t[DPT];
+    }
+      SR_G2(2, false, false)
+    case 48: {  // b / protected(T)
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) t[k] = 1.0f + x[k] * x[k];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_rcp(quad<DPT>(t, h)));
-    } break;
-    case 22:
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_rcp(quad<DPT>(x, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = (x[k] == 0.0f) ? 0.0f : dx[k];
-      break;
-    case 23:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = (fabsf(x[k]) <= 1e-9f) ? 0.0f : -out[k] * out[k];
-      break;
-    case 24:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = signf(x[k]);
-      break;
-    case 25:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = -1.0f;
-      break;
-    case 26: {
-      float t[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) t[k] = 2.0f * out[k];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_rcp(quad<DPT>(t, h)));
-    } break;
-    case 27: {
-      float t[DPT];
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) t[k] = 2.0f * out[k];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(dx, h, v_rcp(quad<DPT>(t, h)));
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = (x[k] == 0.0f) ? 0.0f : signf(x[k]) * dx[k];
-    } break;
-    case 32:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = (x[k] < 80.0f) ? out[k] : 0.0f;
-      break;
-    default:
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) dx[k] = 0.0f;
-      break;
+      for (int k = 0; k < DPT; ++k) {
+        flat[k] = fabsf(T[k]) <= 1e-9f;
+        T[k] = loose_denom(T[k]);
+      }
+    }
+      SR_G2(2, true, false)
+    case 9: SR_G2(1, false, false)
+    case 49: SR_G2(1, true, false)
+    case 10: SR_G1(g_sin)
+    case 11: SR_G1(g_cos)
+    case 12: SR_G1(g_tan)
+    case 13: SR_G1(g_sinh)
+    case 14: SR_G1(g_cosh)
+    case 15: SR_G1(g_tanh)
+    case 16: SR_G1(g_exp)
+    case 17: SR_G1(g_log)
+    case 18: SR_G1(g_rcp)
+    case 19: SR_G1(g_asin)
+    case 20: SR_G1(g_acos)
+    case 21: SR_G1(g_atan)
+    case 22: SR_G1(g_llog)
+    case 23: SR_G1(g_linv)
+    case 24: SR_EACH2(dT[k] = signf(T[k]); T[k] = fabsf(T[k]))
+    case 25: SR_EACH2(T[k] = -T[k]; dT[k] = -1.0f)
+    case 26: SR_G1(g_sqrt)
+    case 27: SR_G1(g_lsqrt)
+    case 32: SR_G1(g_expc)
+    default: SR_EACH2(T[k] = 0.0f; dT[k] = 0.0f; db[k] = 0.0f)
   }
 }
+#undef SR_G1
+#undef SR_G2
+#undef SR_EACH2
 
 // Per-lane FP64 gradient accumulator of constant c: += sum of g over DPT,
 // summed in FP64 (per-datapoint adjoints can be near the FP32 range, where an
@@ -264,6 +363,9 @@ __device__ __forceinline__ void gacc_add(double *gacc, uint32_t c, uint32_t ncon
   gacc[c * 32 + lane] += s;
 }
 
+__device__ __forceinline__ bool needs_db(uint32_t bk) { return bk == kBC || bk == kBS; }
+
+template <bool GTAPE>
 __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjArgs a) {
   constexpr int DPT = kAdjDpt;
   constexpr int TILE = 32 * DPT;
@@ -277,7 +379,8 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
   float *xbuf = reinterpret_cast<float *>(smem_raw);
   float *sreg = xbuf + static_cast<size_t>(kBufs) * rows * span;
   float *tapes = sreg + static_cast<size_t>(W) * p.s_smem * TILE;
-  double *gaccs = reinterpret_cast<double *>(tapes + static_cast<size_t>(W) * a.tape_len * TILE);
+  const size_t smem_tape = GTAPE ? 0 : static_cast<size_t>(W) * a.tape_len * TILE;
+  double *gaccs = reinterpret_cast<double *>(tapes + smem_tape);
   ItemDesc *desc = reinterpret_cast<ItemDesc *>(gaccs + static_cast<size_t>(W) * a.gmax * 32);
   uint64_t *full = reinterpret_cast<uint64_t *>(desc + kBufs);
   uint64_t *empty = full + kBufs;
@@ -299,12 +402,14 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
     return;
   }
 
-  SpillStack st;  // forward spill slots, then adjoint spill slots
+  SpillStack st;  // forward spill slots; adjoint spill slots in the backward sweep
   st.ss = sreg + static_cast<size_t>(warp) * p.s_smem * TILE;
   st.gs = p.spill + (static_cast<size_t>(blockIdx.x) * W + warp) *
                         static_cast<size_t>(p.smax - p.s_smem) * TILE;
   st.s_smem = p.s_smem;
-  float *tape = tapes + static_cast<size_t>(warp) * a.tape_len * TILE;
+  float *tape = GTAPE ? a.gtape + (static_cast<size_t>(blockIdx.x) * W + warp) *
+                                      static_cast<size_t>(a.tape_len) * TILE
+                      : tapes + static_cast<size_t>(warp) * a.tape_len * TILE;
   double *gacc = gaccs + static_cast<size_t>(warp) * a.gmax * 32;
   const int tiles = span / TILE;
   uint32_t buf = 0, phase = 0;
@@ -323,7 +428,9 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
       if (e < 0) break;
       const Instr *code = p.code + p.code_off[e];
       const int len = p.code_len[e];
+      const int lo = a.bwd_lo[e];  // lowest instruction holding a constant (len: none)
       const int nconst = a.const_cnt[e];
+      const int db_base = len - lo;  // tape: dT of [lo, len), then db entries
       for (int c = 0; c < nconst; ++c) gacc[c * 32 + lane] = 0.0;
       double acc = 0.0;
       int cnt = 0;
@@ -331,8 +438,9 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
         const int64_t dp0 = dp_span + static_cast<int64_t>(t) * TILE;
         if (dp0 >= p.N) break;
         const float *xs = xb + t * TILE;
-        // ---- forward, recording every instruction's output ----
+        // ---- forward: values and local partials ----
         float T[DPT];
+        int kb = 0;
         {
           uint4 ins = ldg_instr(code);
           for (int i = 0; i < len; ++i) {
@@ -341,11 +449,17 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
             if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
             if (instr_load(w))
               load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, span, lane, p.cache, p.ldc, dp0);
-            float b[DPT];
+            float b[DPT], dT[DPT], db[DPT];
             const uint32_t bk = instr_b_kind(w);
             if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, span, st, lane, p.cache, p.ldc, dp0);
-            apply_op<DPT>(instr_op(w), T, b);
-            sts_vec<DPT>(tape + i * TILE, lane, T);
+            apply_op_grad<DPT>(instr_op(w), T, b, dT, db);
+            if (i >= lo) {
+              sts_vec<DPT>(tape + (i - lo) * TILE, lane, dT);
+              if (needs_db(bk)) {
+                sts_vec<DPT>(tape + (db_base + kb) * TILE, lane, db);
+                ++kb;
+              }
+            }
             ins = nxt;
           }
         }
@@ -384,46 +498,25 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
           acc += tile_sum;
           cnt += nv;
         }
-        // ---- backward ----
-        for (int i = len - 1; i >= 0; --i) {
+        // ---- backward sweep over the Jacobian tape ----
+        for (int i = len - 1; i >= lo; --i) {
           const uint4 ins = ldg_instr(code + i);
           const uint32_t w = ins.x;
-          const uint32_t op = instr_op(w);
           const uint32_t bk = instr_b_kind(w);
-          float to[DPT], ti[DPT], bv[DPT];
-          lds_vec<DPT>(tape + i * TILE, lane, to);
-          if (instr_load(w))
-            load_leaf<DPT>(instr_leaf_kind(w), ins.y, ti, xs, span, lane, p.cache, p.ldc, dp0);
-          else
-            lds_vec<DPT>(tape + (i - 1) * TILE, lane, ti);
-          if (bk == kBS) {
-            lds_vec<DPT>(tape + ((ins.w >> 20) & 0x3FFu) * TILE, lane, bv);
-          } else if (bk != kBNone) {
-            load_operand<DPT>(bk, ins.z, bv, xs, span, st, lane, p.cache, p.ldc, dp0);
-          } else {
+          float dT[DPT], gi[DPT];
+          lds_vec<DPT>(tape + (i - lo) * TILE, lane, dT);
 #pragma unroll
-            for (int k = 0; k < DPT; ++k) bv[k] = 0.0f;
-          }
-          float dT[DPT], db[DPT];
-          if (bk == kBNone) {
-            unary_partial<DPT>(static_cast<int>(op), ti, to, dT);
+          for (int k = 0; k < DPT; ++k) gi[k] = strong_mul(gT[k], dT[k]);
+          if (needs_db(bk)) {
+            --kb;
+            float db[DPT], gb[DPT];
+            lds_vec<DPT>(tape + (db_base + kb) * TILE, lane, db);
 #pragma unroll
-            for (int k = 0; k < DPT; ++k) db[k] = 0.0f;
-          } else if (op > kOpReversed) {  // T = f(b, T)
-            binary_partials<DPT>(static_cast<int>(op - kOpReversed), bv, ti, to, db, dT);
-          } else {
-            binary_partials<DPT>(static_cast<int>(op), ti, bv, to, dT, db);
-          }
-          float gi[DPT], gb[DPT];
-#pragma unroll
-          for (int k = 0; k < DPT; ++k) {
-            gi[k] = strong_mul(gT[k], dT[k]);
-            gb[k] = strong_mul(gT[k], db[k]);
-          }
-          if (bk == kBC) {
-            gacc_add<DPT>(gacc, (ins.w >> 10) & 0x3FFu, static_cast<uint32_t>(nconst), lane, gb);
-          } else if (bk == kBS) {
-            spill_store<DPT>(st, ins.z, lane, gb);
+            for (int k = 0; k < DPT; ++k) gb[k] = strong_mul(gT[k], db[k]);
+            if (bk == kBC)
+              gacc_add<DPT>(gacc, (ins.w >> 10) & 0x3FFu, static_cast<uint32_t>(nconst), lane, gb);
+            else
+              spill_store<DPT>(st, ins.z, lane, gb);
           }
           if (instr_load(w)) {
             if (instr_leaf_kind(w) == kLeafC)
@@ -513,16 +606,23 @@ __global__ void adam_kernel(int64_t C, const float *__restrict__ grad, float *__
 
 }  // namespace
 
-size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax) {
+size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax,
+                      bool global_tape) {
   const size_t tile = 32u * kAdjDpt;
+  const size_t tape = global_tape ? 0 : static_cast<size_t>(W) * tape_len * tile;
   return (static_cast<size_t>(kBufs) * (V + 1) * span + static_cast<size_t>(W) * s_smem * tile +
-          static_cast<size_t>(W) * tape_len * tile) * sizeof(float) +
+          tape) * sizeof(float) +
          static_cast<size_t>(W) * gmax * 32 * sizeof(double) + kBufs * sizeof(ItemDesc) +
          2 * kBufs * sizeof(uint64_t);
 }
 
-cudaError_t adj_configure(size_t smem, int W, int *blocks_per_sm) {
-  const void *fn = reinterpret_cast<const void *>(&adj_kernel);
+static const void *adj_fn(bool global_tape) {
+  return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true>)
+                     : reinterpret_cast<const void *>(&adj_kernel<false>);
+}
+
+cudaError_t adj_configure(size_t smem, int W, bool global_tape, int *blocks_per_sm) {
+  const void *fn = adj_fn(global_tape);
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;
@@ -531,14 +631,15 @@ cudaError_t adj_configure(size_t smem, int W, int *blocks_per_sm) {
 
 cudaError_t launch_adjoint(const AdjArgs &args, int blocks, size_t smem, cudaStream_t stream) {
   if (args.e.W < 1 || args.e.W > kMaxWarps) return cudaErrorInvalidValue;
+  const bool global_tape = args.gtape != nullptr;
+  const void *fn = adj_fn(global_tape);
   // Each tape class has its own shared-memory size; the attribute is the
   // kernel's, so set it for this launch.
-  const cudaError_t err = cudaFuncSetAttribute(reinterpret_cast<const void *>(&adj_kernel),
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
   if (err != cudaSuccess) return err;
-  adj_kernel<<<blocks, (args.e.W + 1) * 32, smem, stream>>>(args);
-  return cudaGetLastError();
+  void *params[] = {const_cast<AdjArgs *>(&args)};
+  return cudaLaunchKernel(fn, dim3(blocks), dim3((args.e.W + 1) * 32), params, smem, stream);
 }
 
 cudaError_t launch_grad_finalize(const double2 *partial, int n_spans, int E,

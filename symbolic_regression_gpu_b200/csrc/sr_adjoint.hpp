@@ -14,15 +14,18 @@ struct AdjArgs {
   EvalArgs e;                 // forward part (dataset, programs, groups, spans, MSE partials)
   const int64_t *const_off;   // [E] first constant (global index) of each expression
   const int32_t *const_cnt;   // [E] constants of each expression
+  const int32_t *bwd_lo;      // [E] lowest instruction holding a constant (code_len: none)
   double *grad_acc;           // [C] FP64 gradient sums, zeroed before the launch
-  int32_t tape_len;           // tape entries per warp (>= instructions of any program)
+  float *gtape;               // per-warp tapes in global memory, or null (shared memory)
+  int32_t tape_len;           // tape entries per warp (>= the tape of any program)
   int32_t gmax;               // gradient accumulators per warp (>= constants of any program)
 };
 
 // Datapoints per thread of the adjoint kernel.
 int adj_dpt();
-size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax);
-cudaError_t adj_configure(size_t smem, int W, int *blocks_per_sm);
+size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax,
+                      bool global_tape);
+cudaError_t adj_configure(size_t smem, int W, bool global_tape, int *blocks_per_sm);
 cudaError_t launch_adjoint(const AdjArgs &args, int blocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_grad_finalize(const double2 *partial, int n_spans, int E,
                                  const int64_t *const_off, const int32_t *const_cnt,

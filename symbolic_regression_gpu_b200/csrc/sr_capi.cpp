@@ -987,56 +987,95 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop) {
       }
     }
   }
-  // Tape-length classes, each a separate launch with its own tape size.
-  static const int kTapeClasses[] = {8, 16, 32, 64, 128, 256, 512, 1024};
-  std::vector<std::vector<int32_t>> members(8);
+  // Backward range and Jacobian-tape length of each program: the sweep runs
+  // from the last instruction down to the lowest one holding a constant
+  // (lo); the tape holds d out / d T of [lo, len) and d out / d b of the
+  // instructions in that range whose operand b is a constant or a spilled
+  // subtree.
+  SR_TRY_CUDA(ctx, g.h_bwd_lo.ensure(static_cast<size_t>(std::max(E, 1))));
+  std::vector<int32_t> tape_need(static_cast<size_t>(E));
   for (int x = 0; x < E; ++x) {
+    const Instr *code = ps.h_code.p + ps.h_off.p[x];
     const int len = ps.h_len.p[x];
+    int lo = len;
+    for (int i = 0; i < len; ++i) {
+      const Instr &in = code[i];
+      const bool leaf_c = sr::instr_load(in.w) && sr::instr_leaf_kind(in.w) == sr::kLeafC &&
+                          (in.c & 0x3FFu) != sr::kNoConst;
+      const bool b_c = sr::instr_b_kind(in.w) == sr::kBC && ((in.c >> 10) & 0x3FFu) != sr::kNoConst;
+      if (leaf_c || b_c) {
+        lo = i;
+        break;
+      }
+    }
+    int nb = 0;
+    for (int i = lo; i < len; ++i) {
+      const uint32_t bk = sr::instr_b_kind(code[i].w);
+      nb += (bk == sr::kBC || bk == sr::kBS) ? 1 : 0;
+    }
+    g.h_bwd_lo.p[x] = lo;
+    tape_need[static_cast<size_t>(x)] = (len - lo) + nb;
+  }
+  // Tape-length classes, each a separate launch with its own tape size.
+  static const int kTapeClasses[] = {8, 16, 32, 64, 128, 256, 512, 2048};
+  constexpr int kNumClasses = 8;
+  std::vector<std::vector<int32_t>> members(kNumClasses);
+  for (int x = 0; x < E; ++x) {
+    const int need = tape_need[static_cast<size_t>(x)];
     int k = 0;
-    while (k < 7 && len > kTapeClasses[k]) ++k;
+    while (k < kNumClasses - 1 && need > kTapeClasses[k]) ++k;
     members[static_cast<size_t>(k)].push_back(x);
   }
   const int dpt = sr::adj_dpt();
   const int64_t tile = 32 * dpt;
   int dev_max_smem = 0;
   cudaDeviceGetAttribute(&dev_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
-  g.span = static_cast<int>(std::min<int64_t>(512, std::max<int64_t>(tile, round_up(ctx->N, tile))));
+  // One span for every class (the MSE partials are laid out per span): the
+  // largest of 1024 / 512 / 256 / 128 datapoints whose double-buffered X
+  // stage fits in 48 KB.
+  int span = 1024;
+  while (span > tile && 2 * static_cast<int64_t>(ctx->V + 1) * span * 4 > 48 * 1024) span /= 2;
+  g.span = static_cast<int>(std::min<int64_t>(span, std::max<int64_t>(tile, round_up(ctx->N, tile))));
   g.n_spans = (ctx->N == 0) ? 0 : static_cast<int>((ctx->N + g.span - 1) / g.span);
   g.classes.clear();
   std::vector<int32_t> table;
-  int64_t spill_floats = 0;
-  for (int k = 0; k < 8; ++k) {
+  int64_t spill_floats = 0, gtape_floats = 0;
+  const int s_smem = std::min(ps.smax, sr::smem_spill_slots(dpt));
+  for (int k = 0; k < kNumClasses; ++k) {
     auto &mem = members[static_cast<size_t>(k)];
     if (mem.empty()) continue;
     sr::AdjClass cl;
-    int tape_len = 0, cg = 0;
+    int tape_len = 1, cg = 0;
     for (int32_t x : mem) {
-      tape_len = std::max(tape_len, static_cast<int>(ps.h_len.p[x]));
+      tape_len = std::max(tape_len, tape_need[static_cast<size_t>(x)]);
       cg = std::max(cg, ps.n_const[static_cast<size_t>(x)]);
     }
     cl.tape_len = tape_len;
     cl.gmax = std::max(cg, 1);
-    // Largest warp count that keeps two blocks per SM, else one.
-    int best_w = 0, best_b = 0;
+    // Most resident evaluating warps per SM; shared-memory tape if any warp
+    // count fits, else the global tape.
+    int best_w = 0, best_res = 0;
     size_t best_smem = 0;
-    const int s_smem = std::min(ps.smax, sr::smem_spill_slots(dpt));
-    for (int W : {8, 6, 4, 3, 2, 1}) {
-      const size_t smem = sr::adj_smem_bytes(W, ctx->V, s_smem, g.span, cl.tape_len, cl.gmax);
-      if (smem > static_cast<size_t>(dev_max_smem)) continue;
-      int bps = 0;
-      SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, &bps));
-      if (bps <= 0) continue;
-      if (best_w == 0 || (best_b < 2 && bps >= 2) || (bps >= 2 && best_b >= 2 && W * bps > best_w * best_b)) {
-        if (best_w == 0 || bps * W > best_b * best_w || (best_b < 2 && bps >= 2)) {
+    for (int pass = 0; pass < 2 && best_w == 0; ++pass) {
+      const bool gt = (pass == 1);
+      for (int W = sr::kMaxWarps; W >= 1; --W) {
+        const size_t smem =
+            sr::adj_smem_bytes(W, ctx->V, s_smem, g.span, cl.tape_len, cl.gmax, gt);
+        if (smem > static_cast<size_t>(dev_max_smem)) continue;
+        int bps = 0;
+        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, &bps));
+        if (bps <= 0) continue;
+        if (W * bps > best_res) {
+          best_res = W * bps;
           best_w = W;
-          best_b = bps;
           best_smem = smem;
+          cl.global_tape = gt;
         }
       }
     }
     if (best_w == 0)
-      return ctx->fail(SR_ERR_UNSUPPORTED, "programs of " + std::to_string(cl.tape_len) +
-                                               " instructions do not fit the adjoint's tape");
+      return ctx->fail(SR_ERR_UNSUPPORTED, "no adjoint launch shape fits " +
+                                               std::to_string(cl.tape_len) + " tape entries");
     sr::Plan &p = cl.plan;
     p.dpt = dpt;
     p.W = best_w;
@@ -1047,10 +1086,13 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop) {
     p.span = g.span;
     p.n_spans = g.n_spans;
     p.smem = best_smem;
-    p.blocks = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(best_b) * ctx->num_sms,
-                                                  std::max<int64_t>(p.items(), 1)));
+    p.blocks = static_cast<int>(std::min<int64_t>(
+        static_cast<int64_t>(best_res / best_w) * ctx->num_sms, std::max<int64_t>(p.items(), 1)));
     spill_floats = std::max<int64_t>(spill_floats, static_cast<int64_t>(p.blocks) * p.W *
                                                        (p.smax - p.s_smem) * tile);
+    if (cl.global_tape)
+      gtape_floats = std::max<int64_t>(gtape_floats, static_cast<int64_t>(p.blocks) * p.W *
+                                                         cl.tape_len * tile);
     std::stable_sort(mem.begin(), mem.end(), [&](int32_t a, int32_t b) {
       return ps.cost[static_cast<size_t>(a)] > ps.cost[static_cast<size_t>(b)];
     });
@@ -1066,6 +1108,8 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop) {
   SR_TRY_CUDA(ctx, g.groups.ensure(std::max<size_t>(table.size(), 1)));
   SR_TRY_CUDA(ctx, g.const_off.ensure(static_cast<size_t>(E) + 1));
   SR_TRY_CUDA(ctx, g.const_cnt.ensure(static_cast<size_t>(std::max(E, 1))));
+  SR_TRY_CUDA(ctx, g.bwd_lo.ensure(static_cast<size_t>(std::max(E, 1))));
+  if (gtape_floats > 0) SR_TRY_CUDA(ctx, g.gtape.ensure(static_cast<size_t>(gtape_floats)));
   SR_TRY_CUDA(ctx, g.const_loc.ensure(Cs));
   SR_TRY_CUDA(ctx, g.grad_acc.ensure(Cs));
   SR_TRY_CUDA(ctx, g.grad.ensure(Cs));
@@ -1084,6 +1128,8 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop) {
   SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.const_off.p, g.h_const_off.p, (E + 1) * sizeof(int64_t),
                                    cudaMemcpyHostToDevice, s));
   SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.const_cnt.p, g.h_const_cnt.p, E * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, s));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.bwd_lo.p, g.h_bwd_lo.p, E * sizeof(int32_t),
                                    cudaMemcpyHostToDevice, s));
   if (C > 0) {
     SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.const_loc.p, g.h_const_loc.p, C * sizeof(int64_t),
@@ -1117,7 +1163,9 @@ sr_status launch_grad(sr_context *ctx) {
     a.e.group_expr = g.groups.p + cl.group_off;
     a.const_off = g.const_off.p;
     a.const_cnt = g.const_cnt.p;
+    a.bwd_lo = g.bwd_lo.p;
     a.grad_acc = g.grad_acc.p;
+    a.gtape = cl.global_tape ? g.gtape.p : nullptr;
     a.tape_len = cl.tape_len;
     a.gmax = cl.gmax;
     SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));

@@ -130,7 +130,8 @@ struct PlainSet {
 struct AdjClass {
   int tape_len = 0;
   int gmax = 0;
-  int64_t group_off = 0;  // into the concatenated group table
+  bool global_tape = false;  // tape in per-warp global scratch instead of shared memory
+  int64_t group_off = 0;     // into the concatenated group table
   Plan plan;
 };
 
@@ -144,6 +145,9 @@ struct GradSet {
   DevBuf<float> consts;
   DevBuf<float> m, v;
   DevBuf<int32_t> groups;
+  DevBuf<int32_t> bwd_lo;     // [E] lowest instruction holding a constant
+  DevBuf<float> gtape;        // global tapes of classes that do not fit shared memory
+  PinnedBuf<int32_t> h_bwd_lo;
   PinnedBuf<int64_t> h_const_off;
   PinnedBuf<int32_t> h_const_cnt;
   PinnedBuf<int64_t> h_const_loc;

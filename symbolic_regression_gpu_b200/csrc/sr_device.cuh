@@ -158,22 +158,25 @@ __device__ __forceinline__ void stg_vec(float *base, int lane,
         make_float4(v[4 * h + 0], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
 }
 
-// ---- out-of-line 4-wide operator routines ---------------------------------
+// ---- out-of-line operator routines -----------------------------------------
 // Every routine that expands to more than a handful of instructions (CUDA's
 // accurate transcendentals, IEEE division / reciprocal / square root, powf)
-// exists once, four datapoints wide, instead of being inlined DPT times into
-// each opcode of the dispatch switch: that keeps the interpreter's code small
-// enough for the instruction cache.
-#ifndef SR_INLINE_MATH
-#define SR_INLINE_MATH 0
+// exists once, SR_MATH_WIDTH datapoints wide (1, 2 or 4), instead of being
+// inlined DPT times into each opcode of the dispatch switch: that keeps the
+// interpreter's code small enough for the instruction cache.
+#ifndef SR_MATH_WIDTH
+#define SR_MATH_WIDTH 2
 #endif
-#if SR_INLINE_MATH
-#define SR_OUTLINE __forceinline__
-#else
-#define SR_OUTLINE __noinline__
-#endif
+static_assert(SR_MATH_WIDTH == 1 || SR_MATH_WIDTH == 2 || SR_MATH_WIDTH == 4, "width 1, 2 or 4");
 #define SR_V1(NAME, EXPR)                                                   \
-  __device__ SR_OUTLINE float4 NAME(float4 v) {                             \
+  __device__ __noinline__ float NAME##_w1(float x) { return (EXPR); }       \
+  __device__ __noinline__ float2 NAME##_w2(float2 v) {                      \
+    float2 r;                                                               \
+    { const float x = v.x; r.x = (EXPR); }                                  \
+    { const float x = v.y; r.y = (EXPR); }                                  \
+    return r;                                                               \
+  }                                                                         \
+  __device__ __noinline__ float4 NAME##_w4(float4 v) {                      \
     float4 r;                                                               \
     { const float x = v.x; r.x = (EXPR); }                                  \
     { const float x = v.y; r.y = (EXPR); }                                  \
@@ -182,7 +185,14 @@ __device__ __forceinline__ void stg_vec(float *base, int lane,
     return r;                                                               \
   }
 #define SR_V2(NAME, EXPR)                                                   \
-  __device__ SR_OUTLINE float4 NAME(float4 u, float4 v) {                   \
+  __device__ __noinline__ float NAME##_w1(float x, float y) { return (EXPR); } \
+  __device__ __noinline__ float2 NAME##_w2(float2 u, float2 v) {            \
+    float2 r;                                                               \
+    { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
+    { const float x = u.y, y = v.y; r.y = (EXPR); }                         \
+    return r;                                                               \
+  }                                                                         \
+  __device__ __noinline__ float4 NAME##_w4(float4 u, float4 v) {            \
     float4 r;                                                               \
     { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
     { const float x = u.y, y = v.y; r.y = (EXPR); }                         \
@@ -207,6 +217,36 @@ SR_V2(v_div, __fdiv_rn(x, y))
 SR_V2(v_pow, powf(x, y))
 #undef SR_V1
 #undef SR_V2
+
+// Y[k] = FN(X[k]) / Y[k] = FN(X[k], Z[k]) for DPT datapoints through the
+// routine of width SR_MATH_WIDTH (Y may alias X or Z).
+#if SR_MATH_WIDTH == 1
+#define SR_MAP1(FN, Y, X)                                                   \
+  _Pragma("unroll") for (int k_ = 0; k_ < DPT; ++k_) Y[k_] = FN##_w1(X[k_]);
+#define SR_MAP2(FN, Y, X, Z)                                                \
+  _Pragma("unroll") for (int k_ = 0; k_ < DPT; ++k_) Y[k_] = FN##_w1(X[k_], Z[k_]);
+#elif SR_MATH_WIDTH == 2
+#define SR_MAP1(FN, Y, X)                                                   \
+  _Pragma("unroll") for (int k_ = 0; k_ < DPT; k_ += 2) {                   \
+    const float2 r_ = FN##_w2(make_float2(X[k_], X[k_ + 1]));               \
+    Y[k_] = r_.x;                                                           \
+    Y[k_ + 1] = r_.y;                                                       \
+  }
+#define SR_MAP2(FN, Y, X, Z)                                                \
+  _Pragma("unroll") for (int k_ = 0; k_ < DPT; k_ += 2) {                   \
+    const float2 r_ = FN##_w2(make_float2(X[k_], X[k_ + 1]),                \
+                              make_float2(Z[k_], Z[k_ + 1]));               \
+    Y[k_] = r_.x;                                                           \
+    Y[k_ + 1] = r_.y;                                                       \
+  }
+#else
+#define SR_MAP1(FN, Y, X)                                                   \
+  _Pragma("unroll") for (int h_ = 0; h_ < DPT / 4; ++h_)                    \
+      unquad<DPT>(Y, h_, FN##_w4(quad<DPT>(X, h_)));
+#define SR_MAP2(FN, Y, X, Z)                                                \
+  _Pragma("unroll") for (int h_ = 0; h_ < DPT / 4; ++h_)                    \
+      unquad<DPT>(Y, h_, FN##_w4(quad<DPT>(X, h_), quad<DPT>(Z, h_)));
+#endif
 
 template <int DPT>
 __device__ __forceinline__ float4 quad(const float (&v)[DPT], int h) {
@@ -299,17 +339,11 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
     _Pragma("unroll") for (int k = 0; k < DPT; ++k) { STMT; }   \
   }                                                              \
   break;
-#define SR_CALL1(FN)                                                      \
-  {                                                                       \
-    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h)                   \
-        unquad<DPT>(T, h, FN(quad<DPT>(T, h)));                           \
-  }                                                                       \
+#define SR_CALL1(FN) \
+  { SR_MAP1(FN, T, T) } \
   break;
-#define SR_CALL2(FN, X, Y)                                                \
-  {                                                                       \
-    _Pragma("unroll") for (int h = 0; h < DPT / 4; ++h)                   \
-        unquad<DPT>(T, h, FN(quad<DPT>(X, h), quad<DPT>(Y, h)));          \
-  }                                                                       \
+#define SR_CALL2(FN, X, Y) \
+  { SR_MAP2(FN, T, X, Y) } \
   break;
 
 // T = op(T, b) (T = op(T) for unary operators) for DPT datapoints; the
@@ -324,8 +358,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
     case 42: SR_EACH(T[k] = __fsub_rn(b[k], T[k]))
     case 3: SR_EACH(T[k] = __fmul_rn(T[k], b[k]))
     case 4: {  // DIV: NaN when the divisor is 0
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_div(quad<DPT>(T, h), quad<DPT>(b, h)));
+      SR_MAP2(v_div, T, T, b)
 #pragma unroll
       for (int k = 0; k < DPT; ++k) T[k] = (b[k] == 0.0f) ? kNaN : T[k];
     } break;
@@ -333,8 +366,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
       float den[DPT];
 #pragma unroll
       for (int k = 0; k < DPT; ++k) den[k] = T[k];
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_div(quad<DPT>(b, h), quad<DPT>(den, h)));
+      SR_MAP2(v_div, T, b, den)
 #pragma unroll
       for (int k = 0; k < DPT; ++k) T[k] = (den[k] == 0.0f) ? kNaN : T[k];
     } break;
@@ -361,8 +393,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
         z[k] = (T[k] == 0.0f && b[k] == 0.0f);
         T[k] = fabsf(T[k]);
       }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_pow(quad<DPT>(T, h), quad<DPT>(b, h)));
+      SR_MAP2(v_pow, T, T, b)
 #pragma unroll
       for (int k = 0; k < DPT; ++k) T[k] = z[k] ? 0.0f : T[k];
     } break;
@@ -373,8 +404,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
         z[k] = (T[k] == 0.0f && b[k] == 0.0f);
         b[k] = fabsf(b[k]);
       }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_pow(quad<DPT>(b, h), quad<DPT>(T, h)));
+      SR_MAP2(v_pow, T, b, T)
 #pragma unroll
       for (int k = 0; k < DPT; ++k) T[k] = z[k] ? 0.0f : T[k];
     } break;
@@ -397,8 +427,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
         z[k] = (T[k] == 0.0f);
         T[k] = fabsf(T[k]);
       }
-#pragma unroll
-      for (int h = 0; h < DPT / 4; ++h) unquad<DPT>(T, h, v_log(quad<DPT>(T, h)));
+      SR_MAP1(v_log, T, T)
 #pragma unroll
       for (int k = 0; k < DPT; ++k) T[k] = z[k] ? -1e9f : T[k];
     } break;
