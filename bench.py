@@ -46,6 +46,8 @@ def parse_args():
                     help="target CPU work of the CPU-baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the forward+adjoint figures")
     ap.add_argument("--plain-baseline", action="store_true",
                     help="also time the plain per-expression kernel")
     ap.add_argument("--exprs", type=int, default=0,
@@ -243,6 +245,65 @@ def run_reference(args):
 
 # ---- our arm ----------------------------------------------------------------------
 
+def _timed_launches(ev, torch, flush_buf, sr_stream, steps):
+    """Device time (ms) of `steps` launches of the prepared work, L2 flushed
+    before each; CUDA events on the evaluator's stream."""
+    out = []
+    for _ in range(steps):
+        with torch.cuda.stream(sr_stream):
+            flush_buf.fill_(1.0)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(sr_stream)
+        ev.launch()
+        e.record(sr_stream)
+        e.synchronize()
+        out.append(s.elapsed_time(e))
+    return out
+
+
+def adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args):
+    """node-evals/s of the forward pass and of the fused forward + adjoint on
+    the constant-optimisation workload, their cost ratio, and 20 Adam steps."""
+    import torch
+    from symbolic_regression_gpu_b200 import _lib
+    w = make_workload("grad", rank)
+    pop = w.population
+    node_evals = pop.num_tokens * w.num_dps
+    steps = max(3, min(args.steps, 10))
+    ev.set_data(w.X)
+    ev.prepare(pop)
+    _timed_launches(ev, torch, flush_buf, sr_stream, 2)
+    fwd_ms = _timed_launches(ev, torch, flush_buf, sr_stream, steps)
+    res = {"workload": "grad", "exprs": pop.num_exprs, "num_dps": w.num_dps,
+           "num_vars": w.num_vars, "constants": int(np.count_nonzero(pop.tokens == 0)),
+           "fwd": {"value": node_evals / (statistics.mean(fwd_ms) * 1e-3), "unit": UNIT,
+                   "ms": statistics.mean(fwd_ms)}}
+    for name, mode in (("checkpoint", _lib.SR_GRAD_CHECKPOINT),
+                       ("recompute", _lib.SR_GRAD_RECOMPUTE)):
+        try:
+            ev.prepare(pop, gradient=True, grad_mode=mode)
+        except _lib.SrError as ex:
+            res[name] = {"unavailable": str(ex)}
+            continue
+        _timed_launches(ev, torch, flush_buf, sr_stream, 2)
+        ms = _timed_launches(ev, torch, flush_buf, sr_stream, steps)
+        grad = ev.read_grad()
+        res[name] = {"value": node_evals / (statistics.mean(ms) * 1e-3), "unit": UNIT,
+                     "ms": statistics.mean(ms),
+                     "cost_vs_fwd": statistics.mean(ms) / statistics.mean(fwd_ms),
+                     "launches_per_step": int(ev.stats.kernel_launches),
+                     "finite_grad": int(np.isfinite(grad).sum()), "grad_entries": int(grad.size)}
+    mse0 = ev.eval_mse(pop)
+    t0 = time.perf_counter()
+    consts, mse = ev.optimize_constants(pop, steps=20, lr=0.05)
+    res["adam20"] = {"wall_ms": (time.perf_counter() - t0) * 1e3,
+                     "device_ms": float(ev.stats.gpu_kernel_time_ms),
+                     "median_mse_ratio": float(np.nanmedian(mse / mse0)),
+                     "improved_frac": float(np.mean(mse[np.isfinite(mse0)] <=
+                                                    mse0[np.isfinite(mse0)]))}
+    return res
+
+
 def run_ours(args):
     import torch
     rank, local_rank, world = dist_env()
@@ -338,6 +399,12 @@ def run_ours(args):
                  "ms_per_step": statistics.mean(pm)}
         ev.prepare(w.population)
 
+    # Forward + adjoint on the constant-optimisation workload (4,096
+    # expressions with 1-8 constants, 4 variables, 262,144 datapoints).
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args)
+
     # End to end through the public API: pinned host dataset and host
     # population in, MSE vector out, every step.
     Xp = torch.empty(w.X.shape, dtype=torch.float32, pin_memory=True)
@@ -394,6 +461,7 @@ def run_ours(args):
             "gpu_launches": int(st.kernel_launches) * len(step_ms),
             "clocks": clk,
             "plain_kernel": plain,
+            "fwd_adjoint": adjoint,
             "mse_finite": int(np.isfinite(mse).sum()),
         }
         print(json.dumps(line))

@@ -102,6 +102,9 @@ typedef enum sr_status {
 #define SR_EVAL_SUBTREE_CACHE 0x1u /* use the cross-generation subtree cache  */
 #define SR_EVAL_CLEAR_CACHE 0x2u   /* drop the cache first (reference clear_cache) */
 #define SR_EVAL_PLAIN 0x4u         /* plain per-expression kernel (baseline)   */
+#define SR_EVAL_GRADIENT 0x8u      /* sr_prepare: fused forward + adjoint (MSE and
+                                      d MSE / d constants; read with sr_read_grad) */
+#define SR_EVAL_GRAD_RECOMPUTE 0x10u /* with SR_EVAL_GRADIENT: recompute mode      */
 
 typedef struct sr_context sr_context;
 
@@ -223,11 +226,22 @@ sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop,
  * expression i its constants are numbered from const_offsets[i], where
  * const_offsets is the exclusive prefix sum of the per-expression constant
  * counts (sr_count_constants).  grad_out[k] = d mse_i / d c_k. */
-#define SR_GRAD_RECOMPUTE 0 /* forward values recomputed per tile (fused)   */
-#define SR_GRAD_CHECKPOINT 1 /* forward values kept from a separate pass    */
+/* Both modes run forward and backward fused, per tile of datapoints, in one
+ * launch per tape-size class:
+ *   SR_GRAD_CHECKPOINT keeps every instruction's local partials (the Jacobian
+ *     tape) for the tile, in shared memory when it fits, else in per-warp
+ *     global scratch; the backward sweep reads them.
+ *   SR_GRAD_RECOMPUTE keeps only the forward state at segment boundaries and
+ *     recomputes each segment's values and partials during the backward sweep
+ *     (about one more forward pass, a much smaller tape). */
+#define SR_GRAD_RECOMPUTE 0
+#define SR_GRAD_CHECKPOINT 1
 sr_status sr_count_constants(const sr_population *pop, int64_t *const_offsets);
 sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode,
                        float *mse_out, float *grad_out, sr_stats *stats);
+/* After sr_prepare(..., SR_EVAL_GRADIENT) and sr_launch: the gradient of the
+ * last launch (CSR layout above); sr_read_mse gives its MSE. */
+sr_status sr_read_grad(sr_context *ctx, float *grad_out);
 
 /* On-device Adam over every expression's constants (steps iterations of
  * fused forward+adjoint then an Adam update); const_out receives the final

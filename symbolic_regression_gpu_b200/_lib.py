@@ -35,6 +35,8 @@ SR_ERR_TOO_MANY_VARS = 12
 SR_EVAL_SUBTREE_CACHE = 0x1
 SR_EVAL_CLEAR_CACHE = 0x2
 SR_EVAL_PLAIN = 0x4
+SR_EVAL_GRADIENT = 0x8
+SR_EVAL_GRAD_RECOMPUTE = 0x10
 
 # bounds of sr_eval_mse_device_noalloc (include/sr_eval.h)
 SR_NOALLOC_SCRATCH_BYTES = 4 << 20
@@ -139,6 +141,7 @@ _SIGNATURES = {
     "sr_prepare": (c_int32, [c_void_p, _P(sr_population), c_uint32]),
     "sr_launch": (c_int32, [c_void_p]),
     "sr_read_mse": (c_int32, [c_void_p, _P(c_float), _P(sr_stats)]),
+    "sr_read_grad": (c_int32, [c_void_p, _P(c_float)]),
     "sr_device_mse": (c_int32, [c_void_p, _P(c_void_p)]),
     "sr_last_launch_times": (c_int32, [c_void_p, _P(c_float), _P(c_float)]),
     "sr_eval_predictions": (c_int32, [c_void_p, _P(sr_population), c_int64, c_int64, _P(c_float)]),

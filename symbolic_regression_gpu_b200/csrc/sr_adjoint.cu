@@ -77,21 +77,29 @@ struct VD4 {
   float4 v, d;
 };
 
-#define SR_VD1(NAME, VAL, DER)                                       \
-  __device__ __forceinline__ VD1 NAME##_body(float x) {              \
-    const float o = (VAL);                                           \
-    return VD1{o, (DER)};                                            \
-  }                                                                  \
-  __device__ __noinline__ VD1 NAME##_w1(float x) { return NAME##_body(x); } \
+#if SR_ADJ_WIDTH == 1
+#define SR_VD1_WIDE(NAME) \
+  __device__ __noinline__ VD1 NAME##_w1(float x) { return NAME##_body(x); }
+#elif SR_ADJ_WIDTH == 2
+#define SR_VD1_WIDE(NAME)                                            \
   __device__ __noinline__ float4 NAME##_w2(float x0, float x1) {     \
     const VD1 a = NAME##_body(x0), b = NAME##_body(x1);              \
     return make_float4(a.v, a.d, b.v, b.d);                          \
-  }                                                                  \
+  }
+#else
+#define SR_VD1_WIDE(NAME)                                            \
   __device__ __noinline__ VD4 NAME##_w4(float4 x) {                 \
     const VD1 a = NAME##_body(x.x), b = NAME##_body(x.y);            \
     const VD1 c = NAME##_body(x.z), e = NAME##_body(x.w);            \
     return VD4{make_float4(a.v, b.v, c.v, e.v), make_float4(a.d, b.d, c.d, e.d)}; \
   }
+#endif
+#define SR_VD1(NAME, VAL, DER)                                       \
+  __device__ __forceinline__ VD1 NAME##_body(float x) {              \
+    const float o = (VAL);                                           \
+    return VD1{o, (DER)};                                            \
+  }                                                                  \
+  SR_VD1_WIDE(NAME)
 SR_VD1(g_sin, sinf(x), cosf(x))
 SR_VD1(g_cos, cosf(x), -sinf(x))
 SR_VD1(g_tan, tanf(x), __fadd_rn(1.0f, __fmul_rn(o, o)))
@@ -110,6 +118,7 @@ SR_VD1(g_sqrt, __fsqrt_rn(x), __frcp_rn(2.0f * o))
 SR_VD1(g_lsqrt, __fsqrt_rn(fabsf(x)), (x == 0.0f) ? 0.0f : signf(x) * __frcp_rn(2.0f * o))
 SR_VD1(g_expc, expf(fminf(x, 80.0f)), (x < 80.0f) ? o : 0.0f)
 #undef SR_VD1
+#undef SR_VD1_WIDE
 
 // u^v: du = v u^(v-1), dv = u^v ln u.
 __device__ __forceinline__ VD2 g_pow_body(float u, float v) {
@@ -133,15 +142,18 @@ __device__ __forceinline__ VD2 g_div_body(float u, float d, bool flat, bool nan_
   const float rc = __frcp_rn(d);
   return VD2{o, rc, flat ? 0.0f : __fmul_rn(-o, rc)};
 }
+#if SR_ADJ_WIDTH == 1
 __device__ __noinline__ VD2 g_pow_w1(float u, float v) { return g_pow_body(u, v); }
 __device__ __noinline__ VD2 g_lpow_w1(float u, float v) { return g_lpow_body(u, v); }
 __device__ __noinline__ VD2 g_div_w1(float u, float d, bool flat, bool nz) {
   return g_div_body(u, d, flat, nz);
 }
+#endif
 template <int N>
 struct VD2N {
   float v[N], du[N], dv[N];
 };
+#if SR_ADJ_WIDTH == 2
 __device__ __noinline__ VD2N<2> g_pow_w2(float u0, float u1, float v0, float v1) {
   const VD2 a = g_pow_body(u0, v0), b = g_pow_body(u1, v1);
   return VD2N<2>{{a.v, b.v}, {a.du, b.du}, {a.dv, b.dv}};
@@ -155,6 +167,8 @@ __device__ __noinline__ VD2N<2> g_div_w2(float u0, float u1, float d0, float d1,
   const VD2 a = g_div_body(u0, d0, f0, nz), b = g_div_body(u1, d1, f1, nz);
   return VD2N<2>{{a.v, b.v}, {a.du, b.du}, {a.dv, b.dv}};
 }
+#endif
+#if SR_ADJ_WIDTH == 4
 __device__ __noinline__ VD2N<4> g_pow_w4(float4 u, float4 v) {
   const VD2 a = g_pow_body(u.x, v.x), b = g_pow_body(u.y, v.y);
   const VD2 c = g_pow_body(u.z, v.z), e = g_pow_body(u.w, v.w);
@@ -170,6 +184,7 @@ __device__ __noinline__ VD2N<4> g_div_w4(float4 u, float4 d, uint32_t flat, bool
   const VD2 c = g_div_body(u.z, d.z, flat & 4u, nz), e = g_div_body(u.w, d.w, flat & 8u, nz);
   return VD2N<4>{{a.v, b.v, c.v, e.v}, {a.du, b.du, c.du, e.du}, {a.dv, b.dv, c.dv, e.dv}};
 }
+#endif
 
 // T, dT = f(T), f'(T) for DPT datapoints through the routine of width SR_ADJ_WIDTH.
 #if SR_ADJ_WIDTH == 1

@@ -722,6 +722,15 @@ static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint3
   return SR_OK;
 }
 
+}  // extern "C"
+
+namespace {
+sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute);
+sr_status launch_grad(sr_context *ctx);
+}  // namespace
+
+extern "C" {
+
 sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) {
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
@@ -737,7 +746,10 @@ sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) 
   SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
-  if (flags & SR_EVAL_PLAIN) {
+  if (flags & SR_EVAL_GRADIENT) {
+    SR_TRY(prepare_grad(ctx, pop, (flags & SR_EVAL_GRAD_RECOMPUTE) != 0));
+    ctx->mode = sr::Mode::kGrad;
+  } else if (flags & SR_EVAL_PLAIN) {
     SR_TRY(prepare_plain(ctx, pop));
     ctx->mode = sr::Mode::kPlain;
   } else if (flags & SR_EVAL_SUBTREE_CACHE) {
@@ -765,7 +777,10 @@ sr_status sr_launch(sr_context *ctx) {
   cudaStream_t s = ctx->stream;
   SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
   int launches = 0;
-  if (ctx->mode == sr::Mode::kPlain) {
+  if (ctx->mode == sr::Mode::kGrad) {
+    SR_TRY(launch_grad(ctx));
+    launches = static_cast<int>(ctx->grad.classes.size()) + 1;
+  } else if (ctx->mode == sr::Mode::kPlain) {
     SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
     SR_TRY_CUDA(ctx, sr::launch_plain(ctx->plain.tok.p, ctx->plain.val.p, ctx->plain.off.p,
                                       ctx->plain.len.p, ctx->X.p, ctx->ldx, ctx->V, ctx->N,
@@ -846,6 +861,25 @@ sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats) {
   SR_TRY(check_device_error(ctx));
   std::memcpy(mse_out, ctx->h_mse.p, ctx->E * sizeof(float));
   fill_stats(ctx, stats);
+  return SR_OK;
+}
+
+sr_status sr_read_grad(sr_context *ctx, float *grad_out) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (ctx->E == 0) return SR_OK;
+  if (ctx->mode != sr::Mode::kGrad)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "no gradient prepared (SR_EVAL_GRADIENT)");
+  const int64_t C = ctx->grad.C;
+  if (C == 0) return SR_OK;
+  if (!grad_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "grad_out is NULL");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(grad_out, ctx->grad.grad.p, C * sizeof(float),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  SR_TRY(check_device_error(ctx));
+  ctx->prep_stats.d2h_bytes += C * static_cast<int64_t>(sizeof(float));
   return SR_OK;
 }
 
@@ -945,8 +979,10 @@ constexpr int kMaxAdjConsts = 64;  // constants per expression with a gradient
 
 // Compile, lay out constants, split expressions into tape-length classes and
 // upload everything the adjoint launches need.
-sr_status prepare_grad(sr_context *ctx, const sr_population *pop) {
+sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute) {
   sr::GradSet &g = ctx->grad;
+  if (recompute) return ctx->fail(SR_ERR_UNSUPPORTED, "recompute mode not built yet");
+  g.recompute = recompute;
   ProgramSet &ps = ctx->main;
   const int E = pop->num_exprs;
   SR_TRY(compile_set(ctx, E, pop->tokens, pop->values, pop->offsets, nullptr, ps));
@@ -1187,38 +1223,16 @@ sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode, 
   ctx->last_error.clear();
   if (mode != SR_GRAD_CHECKPOINT && mode != SR_GRAD_RECOMPUTE)
     return ctx->fail(SR_ERR_INVALID_ARGUMENT, "unknown gradient mode");
-  if (mode == SR_GRAD_RECOMPUTE)
-    return ctx->fail(SR_ERR_UNSUPPORTED, "recompute mode not built yet");
-  SR_TRY(check_population(ctx, pop));
-  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
-  if (pop->num_exprs == 0) return SR_OK;
-  if (!mse_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "mse_out is NULL");
-  DeviceScope scope(ctx->device);
   const double t0 = now_ms();
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->mode = sr::Mode::kNone;
-  ctx->prep_stats = sr_stats{};
-  ctx->E = pop->num_exprs;
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
-  SR_TRY(prepare_grad(ctx, pop));
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
-  SR_TRY(launch_grad(ctx));
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
-  ctx->timing_valid = true;
-  const int E = pop->num_exprs;
-  const int64_t C = ctx->grad.C;
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_mse.p, ctx->mse.p, E * sizeof(float),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-  if (C > 0 && grad_out)
-    SR_TRY_CUDA(ctx, cudaMemcpyAsync(grad_out, ctx->grad.grad.p, C * sizeof(float),
-                                     cudaMemcpyDeviceToHost, ctx->stream));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  SR_TRY(check_device_error(ctx));
-  std::memcpy(mse_out, ctx->h_mse.p, E * sizeof(float));
-  ctx->prep_stats.kernel_launches = static_cast<int32_t>(ctx->grad.classes.size()) + 1;
+  const uint32_t flags = SR_EVAL_GRADIENT | (mode == SR_GRAD_RECOMPUTE ? SR_EVAL_GRAD_RECOMPUTE : 0u);
+  SR_TRY(sr_prepare(ctx, pop, flags));
+  if (pop->num_exprs == 0) {
+    if (stats) *stats = sr_stats{};
+    return SR_OK;
+  }
+  SR_TRY(sr_launch(ctx));
+  SR_TRY(sr_read_mse(ctx, mse_out, nullptr));
+  if (grad_out) SR_TRY(sr_read_grad(ctx, grad_out));
   if (stats) {
     fill_stats(ctx, stats);
     stats->total_eval_time_ms = now_ms() - t0;
@@ -1232,8 +1246,8 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   if (!adam || adam->steps < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad Adam options");
-  if (adam->mode == SR_GRAD_RECOMPUTE)
-    return ctx->fail(SR_ERR_UNSUPPORTED, "recompute mode not built yet");
+  if (adam->mode != SR_GRAD_CHECKPOINT && adam->mode != SR_GRAD_RECOMPUTE)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "unknown gradient mode");
   SR_TRY(check_population(ctx, pop));
   if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
   if (pop->num_exprs == 0) return SR_OK;
@@ -1244,7 +1258,8 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
   ctx->mode = sr::Mode::kNone;
   ctx->prep_stats = sr_stats{};
   ctx->E = pop->num_exprs;
-  SR_TRY(prepare_grad(ctx, pop));
+  SR_TRY(prepare_grad(ctx, pop, adam->mode == SR_GRAD_RECOMPUTE));
+  ctx->mode = sr::Mode::kGrad;
   sr::GradSet &g = ctx->grad;
   cudaStream_t s = ctx->stream;
   if (g.C > 0) {

@@ -157,9 +157,10 @@ struct GradSet {
   int64_t C = 0;
   int span = 0;
   int n_spans = 0;
+  bool recompute = false;
 };
 
-enum class Mode { kNone, kBatched, kCached, kPlain };
+enum class Mode { kNone, kBatched, kCached, kPlain, kGrad };
 
 }  // namespace sr
 

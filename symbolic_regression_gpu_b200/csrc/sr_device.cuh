@@ -168,14 +168,28 @@ __device__ __forceinline__ void stg_vec(float *base, int lane,
 #define SR_MATH_WIDTH 2
 #endif
 static_assert(SR_MATH_WIDTH == 1 || SR_MATH_WIDTH == 2 || SR_MATH_WIDTH == 4, "width 1, 2 or 4");
+#if SR_MATH_WIDTH == 1
+#define SR_V1(NAME, EXPR) \
+  __device__ __noinline__ float NAME##_w1(float x) { return (EXPR); }
+#define SR_V2(NAME, EXPR) \
+  __device__ __noinline__ float NAME##_w1(float x, float y) { return (EXPR); }
+#elif SR_MATH_WIDTH == 2
 #define SR_V1(NAME, EXPR)                                                   \
-  __device__ __noinline__ float NAME##_w1(float x) { return (EXPR); }       \
   __device__ __noinline__ float2 NAME##_w2(float2 v) {                      \
     float2 r;                                                               \
     { const float x = v.x; r.x = (EXPR); }                                  \
     { const float x = v.y; r.y = (EXPR); }                                  \
     return r;                                                               \
-  }                                                                         \
+  }
+#define SR_V2(NAME, EXPR)                                                   \
+  __device__ __noinline__ float2 NAME##_w2(float2 u, float2 v) {            \
+    float2 r;                                                               \
+    { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
+    { const float x = u.y, y = v.y; r.y = (EXPR); }                         \
+    return r;                                                               \
+  }
+#else
+#define SR_V1(NAME, EXPR)                                                   \
   __device__ __noinline__ float4 NAME##_w4(float4 v) {                      \
     float4 r;                                                               \
     { const float x = v.x; r.x = (EXPR); }                                  \
@@ -185,13 +199,6 @@ static_assert(SR_MATH_WIDTH == 1 || SR_MATH_WIDTH == 2 || SR_MATH_WIDTH == 4, "w
     return r;                                                               \
   }
 #define SR_V2(NAME, EXPR)                                                   \
-  __device__ __noinline__ float NAME##_w1(float x, float y) { return (EXPR); } \
-  __device__ __noinline__ float2 NAME##_w2(float2 u, float2 v) {            \
-    float2 r;                                                               \
-    { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
-    { const float x = u.y, y = v.y; r.y = (EXPR); }                         \
-    return r;                                                               \
-  }                                                                         \
   __device__ __noinline__ float4 NAME##_w4(float4 u, float4 v) {            \
     float4 r;                                                               \
     { const float x = u.x, y = v.x; r.x = (EXPR); }                         \
@@ -200,6 +207,7 @@ static_assert(SR_MATH_WIDTH == 1 || SR_MATH_WIDTH == 2 || SR_MATH_WIDTH == 4, "w
     { const float x = u.w, y = v.w; r.w = (EXPR); }                         \
     return r;                                                               \
   }
+#endif
 SR_V1(v_sin, sinf(x))
 SR_V1(v_cos, cosf(x))
 SR_V1(v_tan, tanf(x))

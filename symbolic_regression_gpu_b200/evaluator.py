@@ -57,6 +57,7 @@ class Evaluator:
         self.num_vars: Optional[int] = None
         self.num_dps: Optional[int] = None
         self._E = 0
+        self._C = 0
 
     # ---- lifecycle -----------------------------------------------------
     def close(self):
@@ -126,11 +127,19 @@ class Evaluator:
         return out
 
     def prepare(self, pop: Population, *, cache: bool = False, clear_cache: bool = False,
-                plain: bool = False):
+                plain: bool = False, gradient: bool = False,
+                grad_mode: int = _lib.SR_GRAD_CHECKPOINT):
+        """Compile and upload `pop` for repeated launch().  gradient=True
+        prepares the fused forward + adjoint (read_mse and read_grad)."""
         cpop = pop.as_c()
-        self._check(_lib.lib.sr_prepare(self._ctx, ctypes.byref(cpop),
-                                        self._flags(cache, clear_cache, plain)), "sr_prepare")
+        flags = self._flags(cache, clear_cache, plain)
+        if gradient:
+            flags = _lib.SR_EVAL_GRADIENT
+            if grad_mode == _lib.SR_GRAD_RECOMPUTE:
+                flags |= _lib.SR_EVAL_GRAD_RECOMPUTE
+        self._check(_lib.lib.sr_prepare(self._ctx, ctypes.byref(cpop), flags), "sr_prepare")
         self._E = pop.num_exprs
+        self._C = int(np.count_nonzero(pop.tokens == 0))
 
     def launch(self):
         """Enqueue the prepared evaluation on the context stream (asynchronous)."""
@@ -141,6 +150,12 @@ class Evaluator:
         self._check(_lib.lib.sr_read_mse(self._ctx, _f32ptr(out), ctypes.byref(self.stats)),
                     "sr_read_mse")
         return out
+
+    def read_grad(self) -> np.ndarray:
+        """d MSE / d constants of the last gradient launch (CSR over expressions)."""
+        out = np.empty(max(self._C, 1), np.float32)
+        self._check(_lib.lib.sr_read_grad(self._ctx, _f32ptr(out)), "sr_read_grad")
+        return out[:self._C]
 
     def last_launch_times(self):
         """(whole launch ms, main interpreter kernel ms) of the last launch."""
