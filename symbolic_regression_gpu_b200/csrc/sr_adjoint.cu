@@ -380,7 +380,74 @@ __device__ __forceinline__ void gacc_add(double *gacc, uint32_t c, uint32_t ncon
 
 __device__ __forceinline__ bool needs_db(uint32_t bk) { return bk == kBC || bk == kBS; }
 
-template <bool GTAPE>
+// One forward instruction: [spill] [T = leaf] [b = operand] T = op(T, b),
+// with its local partials in dT / db.  Returns the operand kind of b.
+template <int DPT>
+__device__ __forceinline__ uint32_t fwd_instr(const uint4 ins, float (&T)[DPT], float (&dT)[DPT],
+                                              float (&db)[DPT], const float *xs, int span,
+                                              const SpillStack &st, int lane, const EvalArgs &p,
+                                              int64_t dp0) {
+  const uint32_t w = ins.x;
+  if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
+  if (instr_load(w))
+    load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, span, lane, p.cache, p.ldc, dp0);
+  float b[DPT];
+  const uint32_t bk = instr_b_kind(w);
+  if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, span, st, lane, p.cache, p.ldc, dp0);
+  apply_op_grad<DPT>(instr_op(w), T, b, dT, db);
+  return bk;
+}
+
+// One backward instruction: gT is the adjoint of the instruction's output
+// on entry and of its input accumulator on exit; db is read only when the
+// operand b is a constant or a spilled subtree.  Adjoint spill slots: `adj`.
+template <int DPT>
+__device__ __forceinline__ void bwd_instr(const uint4 ins, float (&gT)[DPT], const float *dT_at,
+                                          const float *db_at, const SpillStack &adj,
+                                          double *gacc, uint32_t nconst, int lane) {
+  const uint32_t w = ins.x;
+  const uint32_t bk = instr_b_kind(w);
+  float dT[DPT], gi[DPT];
+  lds_vec<DPT>(dT_at, lane, dT);
+#pragma unroll
+  for (int k = 0; k < DPT; ++k) gi[k] = strong_mul(gT[k], dT[k]);
+  if (needs_db(bk)) {
+    float db[DPT], gb[DPT];
+    lds_vec<DPT>(db_at, lane, db);
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) gb[k] = strong_mul(gT[k], db[k]);
+    if (bk == kBC)
+      gacc_add<DPT>(gacc, (ins.w >> 10) & 0x3FFu, nconst, lane, gb);
+    else
+      spill_store<DPT>(adj, ins.z, lane, gb);
+  }
+  if (instr_load(w)) {
+    if (instr_leaf_kind(w) == kLeafC) gacc_add<DPT>(gacc, ins.w & 0x3FFu, nconst, lane, gi);
+    if (instr_spill(w)) {
+      spill_load<DPT>(adj, instr_spill_slot(w), lane, gT);
+    } else {
+#pragma unroll
+      for (int k = 0; k < DPT; ++k) gT[k] = 0.0f;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) gT[k] = gi[k];
+  }
+}
+
+// GTAPE: tapes in per-warp global scratch instead of shared memory.
+// RECOMP: recompute mode.  Checkpoint mode keeps the partials of every
+// instruction in [lo, len) (tape: dT entries, then db entries).  Recompute
+// mode splits the program into segments of kSeg instructions; the forward
+// pass saves T and every forward spill slot at each segment start (after the
+// first) and writes the partials of the last segment only; the backward
+// sweep replays each earlier segment from its checkpoint into the segment
+// tape before sweeping it.  Recompute tape per warp: segment tape (2 seg_cap
+// entries, seg_cap = min(kSeg, longest program of the launch)), adjoint
+// spill slots (smax), checkpoints ((segments - 1) x (1 + smax)).
+constexpr int kSeg = 16;
+
+template <bool GTAPE, bool RECOMP>
 __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjArgs a) {
   constexpr int DPT = kAdjDpt;
   constexpr int TILE = 32 * DPT;
@@ -417,7 +484,7 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
     return;
   }
 
-  SpillStack st;  // forward spill slots; adjoint spill slots in the backward sweep
+  SpillStack st;  // forward spill slots
   st.ss = sreg + static_cast<size_t>(warp) * p.s_smem * TILE;
   st.gs = p.spill + (static_cast<size_t>(blockIdx.x) * W + warp) *
                         static_cast<size_t>(p.smax - p.s_smem) * TILE;
@@ -425,6 +492,17 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
   float *tape = GTAPE ? a.gtape + (static_cast<size_t>(blockIdx.x) * W + warp) *
                                       static_cast<size_t>(a.tape_len) * TILE
                       : tapes + static_cast<size_t>(warp) * a.tape_len * TILE;
+  // Adjoint spill slots: the forward slots in checkpoint mode (forward values
+  // are no longer needed in the sweep); a region of the tape in recompute
+  // mode (the replay needs the forward slots).
+  SpillStack adj = st;
+  float *ckpt = nullptr;
+  if (RECOMP) {
+    adj.ss = tape + 2 * a.seg_cap * TILE;
+    adj.gs = adj.ss;
+    adj.s_smem = p.smax;
+    ckpt = adj.ss + static_cast<size_t>(p.smax) * TILE;
+  }
   double *gacc = gaccs + static_cast<size_t>(warp) * a.gmax * 32;
   const int tiles = span / TILE;
   uint32_t buf = 0, phase = 0;
@@ -444,9 +522,12 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
       const Instr *code = p.code + p.code_off[e];
       const int len = p.code_len[e];
       const int lo = a.bwd_lo[e];  // lowest instruction holding a constant (len: none)
-      const int nconst = a.const_cnt[e];
-      const int db_base = len - lo;  // tape: dT of [lo, len), then db entries
-      for (int c = 0; c < nconst; ++c) gacc[c * 32 + lane] = 0.0;
+      const uint32_t nconst = static_cast<uint32_t>(a.const_cnt[e]);
+      // Checkpoint: partials of [t_lo, len).  Recompute: of the last segment.
+      const int last_seg = RECOMP ? ((len - 1) / kSeg) * kSeg : 0;
+      const int t_lo = RECOMP ? max(lo, last_seg) : lo;
+      const int db_base = RECOMP ? a.seg_cap : len - lo;
+      for (uint32_t c = 0; c < nconst; ++c) gacc[c * 32 + lane] = 0.0;
       double acc = 0.0;
       int cnt = 0;
       for (int t = 0; t < tiles; ++t) {
@@ -460,16 +541,22 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
           uint4 ins = ldg_instr(code);
           for (int i = 0; i < len; ++i) {
             const uint4 nxt = ldg_instr(code + i + 1);
-            const uint32_t w = ins.x;
-            if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
-            if (instr_load(w))
-              load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, span, lane, p.cache, p.ldc, dp0);
-            float b[DPT], dT[DPT], db[DPT];
-            const uint32_t bk = instr_b_kind(w);
-            if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, span, st, lane, p.cache, p.ldc, dp0);
-            apply_op_grad<DPT>(instr_op(w), T, b, dT, db);
-            if (i >= lo) {
-              sts_vec<DPT>(tape + (i - lo) * TILE, lane, dT);
+            if (RECOMP && i > 0 && i % kSeg == 0 && i < last_seg && i + kSeg > lo) {
+              // Checkpoint at the start of a segment the sweep replays (not
+              // the last one, whose partials the forward pass keeps, and only
+              // segments that reach lo).
+              float *ck = ckpt + static_cast<size_t>(i / kSeg - 1) * (1 + p.smax) * TILE;
+              sts_vec<DPT>(ck, lane, T);
+              for (int sl = 0; sl < p.smax; ++sl) {
+                float v[DPT];
+                spill_load<DPT>(st, static_cast<uint32_t>(sl), lane, v);
+                sts_vec<DPT>(ck + (1 + sl) * TILE, lane, v);
+              }
+            }
+            float dT[DPT], db[DPT];
+            const uint32_t bk = fwd_instr<DPT>(ins, T, dT, db, xs, span, st, lane, p, dp0);
+            if (i >= t_lo) {
+              sts_vec<DPT>(tape + (i - (RECOMP ? last_seg : lo)) * TILE, lane, dT);
               if (needs_db(bk)) {
                 sts_vec<DPT>(tape + (db_base + kb) * TILE, lane, db);
                 ++kb;
@@ -513,38 +600,49 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
           acc += tile_sum;
           cnt += nv;
         }
-        // ---- backward sweep over the Jacobian tape ----
-        for (int i = len - 1; i >= lo; --i) {
-          const uint4 ins = ldg_instr(code + i);
-          const uint32_t w = ins.x;
-          const uint32_t bk = instr_b_kind(w);
-          float dT[DPT], gi[DPT];
-          lds_vec<DPT>(tape + (i - lo) * TILE, lane, dT);
-#pragma unroll
-          for (int k = 0; k < DPT; ++k) gi[k] = strong_mul(gT[k], dT[k]);
-          if (needs_db(bk)) {
-            --kb;
-            float db[DPT], gb[DPT];
-            lds_vec<DPT>(tape + (db_base + kb) * TILE, lane, db);
-#pragma unroll
-            for (int k = 0; k < DPT; ++k) gb[k] = strong_mul(gT[k], db[k]);
-            if (bk == kBC)
-              gacc_add<DPT>(gacc, (ins.w >> 10) & 0x3FFu, static_cast<uint32_t>(nconst), lane, gb);
-            else
-              spill_store<DPT>(st, ins.z, lane, gb);
+        // ---- backward sweep ----
+        if (!RECOMP) {
+          for (int i = len - 1; i >= lo; --i) {
+            const uint4 ins = ldg_instr(code + i);
+            if (needs_db(instr_b_kind(ins.x))) --kb;
+            bwd_instr<DPT>(ins, gT, tape + (i - lo) * TILE, tape + (db_base + kb) * TILE, adj,
+                           gacc, nconst, lane);
           }
-          if (instr_load(w)) {
-            if (instr_leaf_kind(w) == kLeafC)
-              gacc_add<DPT>(gacc, ins.w & 0x3FFu, static_cast<uint32_t>(nconst), lane, gi);
-            if (instr_spill(w)) {
-              spill_load<DPT>(st, instr_spill_slot(w), lane, gT);
-            } else {
-#pragma unroll
-              for (int k = 0; k < DPT; ++k) gT[k] = 0.0f;
+        } else {
+          for (int s0 = last_seg; s0 >= 0 && s0 + kSeg > lo; s0 -= kSeg) {
+            const int s1 = min(len, s0 + kSeg);
+            if (s0 != last_seg) {
+              // Replay [s0, s1) from the checkpoint at s0 (s0 > 0: segment 0
+              // starts with a leaf load and needs no state).
+              if (s0 > 0) {
+                const float *ck = ckpt + static_cast<size_t>(s0 / kSeg - 1) * (1 + p.smax) * TILE;
+                lds_vec<DPT>(ck, lane, T);
+                for (int sl = 0; sl < p.smax; ++sl) {
+                  float v[DPT];
+                  lds_vec<DPT>(ck + (1 + sl) * TILE, lane, v);
+                  spill_store<DPT>(st, static_cast<uint32_t>(sl), lane, v);
+                }
+              }
+              kb = 0;
+              for (int i = s0; i < s1; ++i) {
+                const uint4 ins = ldg_instr(code + i);
+                float dT[DPT], db[DPT];
+                const uint32_t bk = fwd_instr<DPT>(ins, T, dT, db, xs, span, st, lane, p, dp0);
+                if (i >= lo) {
+                  sts_vec<DPT>(tape + (i - s0) * TILE, lane, dT);
+                  if (needs_db(bk)) {
+                    sts_vec<DPT>(tape + (db_base + kb) * TILE, lane, db);
+                    ++kb;
+                  }
+                }
+              }
             }
-          } else {
-#pragma unroll
-            for (int k = 0; k < DPT; ++k) gT[k] = gi[k];
+            for (int i = s1 - 1; i >= max(s0, lo); --i) {
+              const uint4 ins = ldg_instr(code + i);
+              if (needs_db(instr_b_kind(ins.x))) --kb;
+              bwd_instr<DPT>(ins, gT, tape + (i - s0) * TILE, tape + (db_base + kb) * TILE, adj,
+                             gacc, nconst, lane);
+            }
           }
         }
       }
@@ -557,7 +655,7 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
         p.partial[static_cast<int64_t>(d.span) * p.E + e] =
             make_double2(acc, static_cast<double>(cnt));
       const int64_t coff = a.const_off[e];
-      for (int c = 0; c < nconst; ++c) {
+      for (uint32_t c = 0; c < nconst; ++c) {
         double g = gacc[c * 32 + lane];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
@@ -631,23 +729,27 @@ size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax
          2 * kBufs * sizeof(uint64_t);
 }
 
-static const void *adj_fn(bool global_tape) {
-  return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true>)
-                     : reinterpret_cast<const void *>(&adj_kernel<false>);
+static const void *adj_fn(bool global_tape, bool recompute) {
+  if (recompute)
+    return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true, true>)
+                       : reinterpret_cast<const void *>(&adj_kernel<false, true>);
+  return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true, false>)
+                     : reinterpret_cast<const void *>(&adj_kernel<false, false>);
 }
 
-cudaError_t adj_configure(size_t smem, int W, bool global_tape, int *blocks_per_sm) {
-  const void *fn = adj_fn(global_tape);
+cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute,
+                          int *blocks_per_sm) {
+  const void *fn = adj_fn(global_tape, recompute);
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, (W + 1) * 32, smem);
 }
 
-cudaError_t launch_adjoint(const AdjArgs &args, int blocks, size_t smem, cudaStream_t stream) {
+cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int blocks, size_t smem,
+                           cudaStream_t stream) {
   if (args.e.W < 1 || args.e.W > kMaxWarps) return cudaErrorInvalidValue;
-  const bool global_tape = args.gtape != nullptr;
-  const void *fn = adj_fn(global_tape);
+  const void *fn = adj_fn(args.gtape != nullptr, recompute);
   // Each tape class has its own shared-memory size; the attribute is the
   // kernel's, so set it for this launch.
   const cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -656,6 +758,8 @@ cudaError_t launch_adjoint(const AdjArgs &args, int blocks, size_t smem, cudaStr
   void *params[] = {const_cast<AdjArgs *>(&args)};
   return cudaLaunchKernel(fn, dim3(blocks), dim3((args.e.W + 1) * 32), params, smem, stream);
 }
+
+int adj_segment() { return kSeg; }
 
 cudaError_t launch_grad_finalize(const double2 *partial, int n_spans, int E,
                                  const int64_t *const_off, const int32_t *const_cnt,

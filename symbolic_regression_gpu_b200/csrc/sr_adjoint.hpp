@@ -19,14 +19,20 @@ struct AdjArgs {
   float *gtape;               // per-warp tapes in global memory, or null (shared memory)
   int32_t tape_len;           // tape entries per warp (>= the tape of any program)
   int32_t gmax;               // gradient accumulators per warp (>= constants of any program)
+  int32_t seg_cap;            // recompute mode: segment-tape entries (min(segment, longest))
+  int32_t reserved0;
 };
 
 // Datapoints per thread of the adjoint kernel.
 int adj_dpt();
 size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax,
                       bool global_tape);
-cudaError_t adj_configure(size_t smem, int W, bool global_tape, int *blocks_per_sm);
-cudaError_t launch_adjoint(const AdjArgs &args, int blocks, size_t smem, cudaStream_t stream);
+// Instructions per recompute segment.
+int adj_segment();
+cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute,
+                          int *blocks_per_sm);
+cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int blocks, size_t smem,
+                           cudaStream_t stream);
 cudaError_t launch_grad_finalize(const double2 *partial, int n_spans, int E,
                                  const int64_t *const_off, const int32_t *const_cnt,
                                  const double *grad_acc, float *mse, float *grad,

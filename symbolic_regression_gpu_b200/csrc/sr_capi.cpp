@@ -981,7 +981,6 @@ constexpr int kMaxAdjConsts = 64;  // constants per expression with a gradient
 // upload everything the adjoint launches need.
 sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute) {
   sr::GradSet &g = ctx->grad;
-  if (recompute) return ctx->fail(SR_ERR_UNSUPPORTED, "recompute mode not built yet");
   g.recompute = recompute;
   ProgramSet &ps = ctx->main;
   const int E = pop->num_exprs;
@@ -1050,7 +1049,15 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
       nb += (bk == sr::kBC || bk == sr::kBS) ? 1 : 0;
     }
     g.h_bwd_lo.p[x] = lo;
-    tape_need[static_cast<size_t>(x)] = (len - lo) + nb;
+    if (recompute) {
+      // Segment tape, adjoint spill slots, checkpoints.
+      const int seg = sr::adj_segment();
+      const int nseg = (len + seg - 1) / seg;
+      tape_need[static_cast<size_t>(x)] =
+          2 * std::min(seg, len) + ps.smax + std::max(nseg - 1, 0) * (1 + ps.smax);
+    } else {
+      tape_need[static_cast<size_t>(x)] = (len - lo) + nb;
+    }
   }
   // Tape-length classes, each a separate launch with its own tape size.
   static const int kTapeClasses[] = {8, 16, 32, 64, 128, 256, 512, 2048};
@@ -1082,10 +1089,13 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     if (mem.empty()) continue;
     sr::AdjClass cl;
     int tape_len = 1, cg = 0;
+    int maxlen = 1;
     for (int32_t x : mem) {
       tape_len = std::max(tape_len, tape_need[static_cast<size_t>(x)]);
       cg = std::max(cg, ps.n_const[static_cast<size_t>(x)]);
+      maxlen = std::max(maxlen, static_cast<int>(ps.h_len.p[x]));
     }
+    cl.seg_cap = std::min(sr::adj_segment(), maxlen);
     cl.tape_len = tape_len;
     cl.gmax = std::max(cg, 1);
     // Most resident evaluating warps per SM; shared-memory tape if any warp
@@ -1099,7 +1109,7 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
             sr::adj_smem_bytes(W, ctx->V, s_smem, g.span, cl.tape_len, cl.gmax, gt);
         if (smem > static_cast<size_t>(dev_max_smem)) continue;
         int bps = 0;
-        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, &bps));
+        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, &bps));
         if (bps <= 0) continue;
         if (W * bps > best_res) {
           best_res = W * bps;
@@ -1203,9 +1213,10 @@ sr_status launch_grad(sr_context *ctx) {
     a.grad_acc = g.grad_acc.p;
     a.gtape = cl.global_tape ? g.gtape.p : nullptr;
     a.tape_len = cl.tape_len;
+    a.seg_cap = cl.seg_cap;
     a.gmax = cl.gmax;
     SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, cl.plan.blocks, cl.plan.smem, s));
+    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.blocks, cl.plan.smem, s));
   }
   SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
   SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E, g.const_off.p,

@@ -131,6 +131,7 @@ struct AdjClass {
   int tape_len = 0;
   int gmax = 0;
   bool global_tape = false;  // tape in per-warp global scratch instead of shared memory
+  int seg_cap = 0;           // recompute mode: segment-tape entries
   int64_t group_off = 0;     // into the concatenated group table
   Plan plan;
 };

@@ -217,3 +217,45 @@ def test_adam_lowers_mse_and_writes_constants_back(evaluator):
     seeded = np.arange(0, pop.num_exprs, 4)
     assert np.median(mse[seeded] / mse0[seeded]) < 0.5
     assert np.mean(mse[fin] <= mse0[fin] * (1 + 1e-6)) > 0.8
+
+
+def _ulps(a, b):
+    a = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    b = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    a = np.where(a < 0, -(a & 0x7FFFFFFF), a)
+    b = np.where(b < 0, -(b & 0x7FFFFFFF), b)
+    return np.abs(a - b)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_recompute_matches_checkpoint(evaluator, seed):
+    # Same values and partials, same sweep order: identical MSE, gradients
+    # equal up to the order of the FP64 atomic adds across spans (<= 2 ulp of
+    # the FP32 result).  Long programs give several segments, with spills.
+    rng = np.random.default_rng(70 + seed)
+    V, N = 4, 5_000
+    X = _dataset(rng, V, N)
+    gen = synth.TreeGen(rng, V, p_const=0.35, binary=(1, 2, 3, 4, 6, 7, 8),
+                        unary=(10, 11, 15, 21, 25, 32, 22, 27))
+    exprs = [gen.depth_tree(5, full=False) for _ in range(200)]
+    exprs += [gen.sized_tree(int(L)) for L in rng.integers(40, 400, size=40)]
+    pop = Population.from_lists(exprs)
+    evaluator.set_data(X)
+    m_c, g_c = evaluator.eval_grad(pop, mode=_lib.SR_GRAD_CHECKPOINT)
+    m_r, g_r = evaluator.eval_grad(pop, mode=_lib.SR_GRAD_RECOMPUTE)
+    assert np.array_equal(m_c, m_r, equal_nan=True)
+    assert np.array_equal(np.isfinite(g_c), np.isfinite(g_r))
+    fin = np.isfinite(g_c)
+    assert _ulps(g_c[fin], g_r[fin]).max() <= 2
+
+
+def test_recompute_adam(evaluator):
+    w = synth.grad_workload(seed=11, E=128, N=20_000)
+    evaluator.set_data(w.X)
+    mse0 = evaluator.eval_mse(w.population)
+    c_c, m_c = evaluator.optimize_constants(w.population, steps=5, mode=_lib.SR_GRAD_CHECKPOINT)
+    c_r, m_r = evaluator.optimize_constants(w.population, steps=5, mode=_lib.SR_GRAD_RECOMPUTE)
+    fin = np.isfinite(m_c) & np.isfinite(m_r)
+    np.testing.assert_allclose(m_r[fin], m_c[fin], rtol=1e-4)
+    seeded = np.arange(0, w.population.num_exprs, 4)
+    assert np.median(m_r[seeded] / mse0[seeded]) < 1.0
