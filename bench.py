@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--warps", type=int, default=0, help="force evaluating warps per block")
     ap.add_argument("--profile-launch", action="store_true",
                     help="prepare and run a single evaluation, no timing (for ncu)")
+    ap.add_argument("--grad-mode", choices=["none", "checkpoint", "recompute"], default="none",
+                    help="with --profile-launch: run the fused forward + adjoint instead")
     return ap.parse_args()
 
 
@@ -74,15 +76,21 @@ def make_workload(name: str, rank: int, exprs: int = 0):
 
 def profile_launch(args):
     """One prepared evaluation on GPU 0, nothing timed (the ncu capture case)."""
-    from symbolic_regression_gpu_b200 import Evaluator
+    from symbolic_regression_gpu_b200 import Evaluator, _lib
     w = make_workload(args.workload, 0, args.exprs)
     with Evaluator(device=0, dpt=args.dpt, warps_per_block=args.warps) as ev:
         ev.set_data(w.X)
-        ev.prepare(w.population)
+        if args.grad_mode == "none":
+            ev.prepare(w.population)
+        else:
+            mode = (_lib.SR_GRAD_CHECKPOINT if args.grad_mode == "checkpoint"
+                    else _lib.SR_GRAD_RECOMPUTE)
+            ev.prepare(w.population, gradient=True, grad_mode=mode)
         ev.launch()
         mse = ev.read_mse()
         st = ev.stats
-        print(json.dumps({"workload": w.name, "exprs": w.population.num_exprs,
+        print(json.dumps({"workload": w.name, "grad_mode": args.grad_mode,
+                          "exprs": w.population.num_exprs,
                           "num_dps": w.num_dps, "dpt": st.dpt,
                           "warps_per_block": st.warps_per_block, "blocks": st.blocks,
                           "work_items": st.work_items, "kernel_ms": st.eval_kernel_time_ms,
@@ -315,7 +323,7 @@ def run_ours(args):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
 
-    from symbolic_regression_gpu_b200 import Evaluator
+    from symbolic_regression_gpu_b200 import Evaluator, sharding
 
     w = make_workload(args.workload, rank, args.exprs)
     flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -409,12 +417,18 @@ def run_ours(args):
     # population in, MSE vector out, every step.
     Xp = torch.empty(w.X.shape, dtype=torch.float32, pin_memory=True)
     Xp.numpy()[...] = w.X
+    # With N ranks the population is the concatenation of the ranks' slices;
+    # every rank ends the step holding the MSE of all of it (one all-gather,
+    # as the selection step of the evolution loop needs).
+    bounds = np.arange(world + 1, dtype=np.int64) * w.population.num_exprs
     e2e_times, h2d, d2h = [], 0, 0
     for k in range(args.e2e_steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ev.set_data(Xp.numpy())
         out = ev.eval_mse(w.population)
+        if world > 1:
+            out = sharding.gather_mse(out, bounds, device=dev)
         dt = time.perf_counter() - t0
         if k > 0:
             e2e_times.append(dt)

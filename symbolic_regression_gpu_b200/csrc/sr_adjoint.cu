@@ -100,8 +100,20 @@ struct VD4 {
     return VD1{o, (DER)};                                            \
   }                                                                  \
   SR_VD1_WIDE(NAME)
-SR_VD1(g_sin, sinf(x), cosf(x))
-SR_VD1(g_cos, cosf(x), -sinf(x))
+// sin and cos share one argument reduction through sincosf (its two results
+// are bit-identical to sinf / cosf over every float input on sm_100a).
+__device__ __forceinline__ VD1 g_sin_body(float x) {
+  float s, c;
+  sincosf(x, &s, &c);
+  return VD1{s, c};
+}
+SR_VD1_WIDE(g_sin)
+__device__ __forceinline__ VD1 g_cos_body(float x) {
+  float s, c;
+  sincosf(x, &s, &c);
+  return VD1{c, -s};
+}
+SR_VD1_WIDE(g_cos)
 SR_VD1(g_tan, tanf(x), __fadd_rn(1.0f, __fmul_rn(o, o)))
 SR_VD1(g_sinh, sinhf(x), coshf(x))
 SR_VD1(g_cosh, coshf(x), sinhf(x))
