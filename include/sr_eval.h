@@ -229,8 +229,9 @@ sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop,
 /* Both modes run forward and backward fused, per tile of datapoints, in one
  * launch per tape-size class:
  *   SR_GRAD_CHECKPOINT keeps every instruction's local partials (the Jacobian
- *     tape) for the tile, in shared memory when it fits, else in per-warp
- *     global scratch; the backward sweep reads them.
+ *     tape) for the tile, in shared memory, or in per-warp global scratch
+ *     (L2-resident) when that keeps more warps resident; the backward sweep
+ *     reads them.
  *   SR_GRAD_RECOMPUTE keeps only the forward state at segment boundaries and
  *     recomputes each segment's values and partials during the backward sweep
  *     (about one more forward pass, a much smaller tape). */

@@ -1098,11 +1098,16 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     cl.seg_cap = std::min(sr::adj_segment(), maxlen);
     cl.tape_len = tape_len;
     cl.gmax = std::max(cg, 1);
-    // Most resident evaluating warps per SM; shared-memory tape if any warp
-    // count fits, else the global tape.
+    // Most resident evaluating warps per SM.  A shared-memory tape costs
+    // occupancy (every warp holds its whole tape), a global one costs L2
+    // traffic (each tape entry is written and read back once per tile, by the
+    // same warp, so it stays in L2 while the resident tapes fit there): the
+    // global tape is taken only when it gives strictly more resident warps
+    // and the resident tapes stay within kL2TapeBytes.
+    constexpr int64_t kL2TapeBytes = 64ll << 20;
     int best_w = 0, best_res = 0;
     size_t best_smem = 0;
-    for (int pass = 0; pass < 2 && best_w == 0; ++pass) {
+    for (int pass = 0; pass < 2; ++pass) {
       const bool gt = (pass == 1);
       for (int W = sr::kMaxWarps; W >= 1; --W) {
         const size_t smem =
@@ -1111,6 +1116,9 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
         int bps = 0;
         SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, &bps));
         if (bps <= 0) continue;
+        const int64_t resident_tape =
+            static_cast<int64_t>(W) * bps * ctx->num_sms * cl.tape_len * tile * 4;
+        if (gt && best_w != 0 && resident_tape > kL2TapeBytes) continue;
         if (W * bps > best_res) {
           best_res = W * bps;
           best_w = W;
