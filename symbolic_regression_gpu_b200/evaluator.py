@@ -62,7 +62,11 @@ class Evaluator:
     # ---- lifecycle -----------------------------------------------------
     def close(self):
         if getattr(self, "_ctx", None):
-            _lib.lib.sr_destroy(self._ctx)
+            # At interpreter shutdown the module globals may already be gone;
+            # the process exit then releases the context with the device.
+            lib = getattr(_lib, "lib", None) if _lib is not None else None
+            if lib is not None:
+                lib.sr_destroy(self._ctx)
             self._ctx = None
 
     def __del__(self):
