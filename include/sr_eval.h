@@ -115,9 +115,12 @@ typedef struct sr_options {
   int32_t min_subtree_size; /* detection min size; reference 3 (cl_gpu_eval.cu:373) */
   int32_t min_subtree_freq; /* detection min frequency; reference 10 (same line) */
   int32_t dpt;              /* datapoints per thread: 0 = tuned, 4, 8 or 16   */
-  int32_t warps_per_block;  /* evaluating warps per block: 0 = tuned, 1..8     */
+  int32_t warps_per_block;  /* evaluating warps per block: 0 = tuned, 1..16    */
   int32_t autotune;         /* 1 = time candidate launch shapes on first use  */
-  int32_t use_graphs;       /* 1 = replay each launch shape from a CUDA graph */
+  int32_t use_graphs;       /* 1 = sr_launch captures the prepared launch
+                               sequence (memsets, kernels, timing events) in
+                               a CUDA graph on first use and replays it until
+                               the next sr_prepare / sr_set_data            */
   int32_t host_threads;     /* host compile threads; 0 = hardware concurrency  */
   int32_t reserved0;
   const char *tune_cache_path; /* JSON file for tuned shapes; NULL = none      */

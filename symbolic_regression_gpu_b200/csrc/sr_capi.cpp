@@ -383,6 +383,26 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
 }  // namespace
 
 // ============================================================================
+// Record timing event k on the context stream.  While sr_launch captures a
+// graph the event is recorded as an external event, which makes it an
+// event-record node of the graph (a plain record would only mark a capture
+// dependency); outside capture that flag is not accepted.
+static cudaError_t record_event(sr_context *ctx, int k) {
+  return ctx->capturing ? cudaEventRecordWithFlags(ctx->ev[k], ctx->stream, cudaEventRecordExternal)
+                        : cudaEventRecord(ctx->ev[k], ctx->stream);
+}
+
+// Forget the prepared launch (and its captured graph, whose kernel arguments
+// point into buffers that the next prepare / set_data may move).
+static void reset_prepared(sr_context *ctx) {
+  ctx->mode = sr::Mode::kNone;
+  if (ctx->graph_exec) {
+    cudaGraphExecDestroy(ctx->graph_exec);
+    ctx->graph_exec = nullptr;
+  }
+  ctx->graph_launches = 0;
+}
+
 extern "C" {
 
 int32_t sr_abi_version(void) { return SR_ABI_VERSION; }
@@ -481,6 +501,7 @@ sr_status sr_destroy(sr_context *ctx) {
   if (!ctx) return SR_OK;
   DeviceScope scope(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  reset_prepared(ctx);
   for (auto &ev : ctx->ev)
     if (ev) cudaEventDestroy(ev);
   if (ctx->d_counter) cudaFree(ctx->d_counter);
@@ -514,7 +535,7 @@ sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, in
   ctx->V = num_vars;
   ctx->N = num_dps;
   ctx->cache.clear();  // cached subtree values belong to the old data
-  ctx->mode = sr::Mode::kNone;
+  reset_prepared(ctx);
   return SR_OK;
 }
 
@@ -550,7 +571,7 @@ static sr_status set_data_host(sr_context *ctx, const float *X, const float *con
   ctx->V = num_vars;
   ctx->N = num_dps;
   ctx->cache.clear();
-  ctx->mode = sr::Mode::kNone;
+  reset_prepared(ctx);
   return SR_OK;
 }
 
@@ -738,7 +759,7 @@ sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) 
   if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->mode = sr::Mode::kNone;
+  reset_prepared(ctx);
   ctx->prep_stats = sr_stats{};
   const int E = pop->num_exprs;
   ctx->E = E;
@@ -769,24 +790,21 @@ sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) 
   return SR_OK;
 }
 
-sr_status sr_launch(sr_context *ctx) {
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  if (ctx->E == 0) return SR_OK;
-  if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing prepared");
-  DeviceScope scope(ctx->device);
+// Enqueue the prepared launch sequence on the context stream.
+static sr_status enqueue_launch(sr_context *ctx, int *launches_out) {
   cudaStream_t s = ctx->stream;
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+  SR_TRY_CUDA(ctx, record_event(ctx, 0));
   int launches = 0;
   if (ctx->mode == sr::Mode::kGrad) {
     SR_TRY(launch_grad(ctx));
     launches = static_cast<int>(ctx->grad.classes.size()) + 1;
   } else if (ctx->mode == sr::Mode::kPlain) {
-    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    SR_TRY_CUDA(ctx, record_event(ctx, 1));
     SR_TRY_CUDA(ctx, sr::launch_plain(ctx->plain.tok.p, ctx->plain.val.p, ctx->plain.off.p,
                                       ctx->plain.len.p, ctx->X.p, ctx->ldx, ctx->V, ctx->N,
                                       ctx->plain.E, ctx->partial.p, ctx->plain.n_dpblocks, s));
     launches += ctx->N > 0 ? 1 : 0;
-    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+    SR_TRY_CUDA(ctx, record_event(ctx, 2));
     SR_TRY_CUDA(ctx, sr::launch_finalize(ctx->partial.p, ctx->N > 0 ? ctx->plain.n_dpblocks : 0,
                                          ctx->E, ctx->mse.p, s));
     ++launches;
@@ -796,17 +814,53 @@ sr_status sr_launch(sr_context *ctx) {
                         ctx->sub.row.p));
       ++launches;
     }
-    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+    SR_TRY_CUDA(ctx, record_event(ctx, 1));
     if (ctx->main.plan.items() > 0) {
       SR_TRY(launch_set(ctx, ctx->main, false, ctx->d_counter, nullptr, 0, nullptr));
       ++launches;
     }
-    SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+    SR_TRY_CUDA(ctx, record_event(ctx, 2));
     SR_TRY_CUDA(ctx, sr::launch_finalize(ctx->partial.p, ctx->main.plan.n_spans, ctx->E,
                                          ctx->mse.p, s));
     ++launches;
   }
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[3], s));
+  SR_TRY_CUDA(ctx, record_event(ctx, 3));
+  *launches_out = launches;
+  return SR_OK;
+}
+
+sr_status sr_launch(sr_context *ctx) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (ctx->E == 0) return SR_OK;
+  if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing prepared");
+  DeviceScope scope(ctx->device);
+  cudaStream_t s = ctx->stream;
+  int launches = 0;
+  if (ctx->opts.use_graphs) {
+    if (!ctx->graph_exec) {
+      // Relaxed mode: the launchers set kernel attributes while capturing.
+      SR_TRY_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+      ctx->capturing = true;
+      const sr_status st = enqueue_launch(ctx, &launches);
+      ctx->capturing = false;
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (st != SR_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+      }
+      SR_TRY_CUDA(ctx, ce);
+      const cudaError_t ie = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) ctx->graph_exec = nullptr;
+      SR_TRY_CUDA(ctx, ie);
+      ctx->graph_launches = launches;
+    }
+    SR_TRY_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, s));
+    launches = ctx->graph_launches;
+  } else {
+    SR_TRY(enqueue_launch(ctx, &launches));
+  }
   ctx->timing_valid = true;
   ctx->prep_stats.kernel_launches = launches;
   return SR_OK;
@@ -933,7 +987,7 @@ sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop, int64_t
     return ctx->fail(SR_ERR_UNSUPPORTED, "prediction buffer would exceed 16 GiB");
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->mode = sr::Mode::kNone;
+  reset_prepared(ctx);
   SR_TRY(compile_set(ctx, E, pop->tokens, pop->values, pop->offsets, nullptr, ctx->main));
   SR_TRY_CUDA(ctx, ctx->main.h_row.ensure(static_cast<size_t>(E)));
   for (int x = 0; x < E; ++x) ctx->main.h_row.p[x] = x;
@@ -1202,7 +1256,7 @@ sr_status launch_grad(sr_context *ctx) {
   ProgramSet &ps = ctx->main;
   cudaStream_t s = ctx->stream;
   if (g.C > 0) SR_TRY_CUDA(ctx, cudaMemsetAsync(g.grad_acc.p, 0, g.C * sizeof(double), s));
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+  SR_TRY_CUDA(ctx, record_event(ctx, 1));
   for (const sr::AdjClass &cl : g.classes) {
     if (cl.plan.items() == 0) continue;
     sr::AdjArgs a{};
@@ -1226,7 +1280,7 @@ sr_status launch_grad(sr_context *ctx) {
     SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
     SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.blocks, cl.plan.smem, s));
   }
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+  SR_TRY_CUDA(ctx, record_event(ctx, 2));
   SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E, g.const_off.p,
                                             g.const_cnt.p, g.grad_acc.p, ctx->mse.p, g.grad.p, s));
   return SR_OK;
@@ -1274,7 +1328,7 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
   DeviceScope scope(ctx->device);
   const double t0 = now_ms();
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->mode = sr::Mode::kNone;
+  reset_prepared(ctx);
   ctx->prep_stats = sr_stats{};
   ctx->E = pop->num_exprs;
   SR_TRY(prepare_grad(ctx, pop, adam->mode == SR_GRAD_RECOMPUTE));

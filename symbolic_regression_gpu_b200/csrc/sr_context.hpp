@@ -209,6 +209,12 @@ struct sr_context {
 
   // timing
   cudaEvent_t ev[6] = {};
+  // use_graphs: the prepared launch sequence as an instantiated CUDA graph,
+  // captured on the first sr_launch after a prepare and replayed until the
+  // next prepare / set_data (which destroy it: buffers may move).
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0;
+  bool capturing = false;  // sr_launch is capturing graph_exec
   bool timing_valid = false;
 
   // statistics of the prepared population

@@ -35,7 +35,7 @@ class Evaluator:
     def __init__(self, device: int = -1, *, cache_capacity: int = 2048,
                  min_subtree_size: int = 3, min_subtree_freq: int = 10, dpt: int = 0,
                  warps_per_block: int = 0, autotune: bool = False, host_threads: int = 0,
-                 tune_cache_path: Optional[str] = None, stream=None):
+                 tune_cache_path: Optional[str] = None, stream=None, use_graphs: bool = False):
         opts = _lib.sr_options()
         _lib.check(_lib.lib.sr_options_init(ctypes.byref(opts)))
         opts.device = device
@@ -45,6 +45,7 @@ class Evaluator:
         opts.dpt = dpt
         opts.warps_per_block = warps_per_block
         opts.autotune = 1 if autotune else 0
+        opts.use_graphs = 1 if use_graphs else 0
         opts.host_threads = host_threads
         self._tune_path = tune_cache_path.encode() if tune_cache_path else None
         opts.tune_cache_path = self._tune_path
