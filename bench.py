@@ -48,6 +48,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the forward+adjoint figures")
+    ap.add_argument("--no-cache-figures", action="store_true",
+                    help="skip the subtree-cache figures")
+    ap.add_argument("--large", action="store_true",
+                    help="also run the 100,000 x 4M population (about two minutes)")
     ap.add_argument("--plain-baseline", action="store_true",
                     help="also time the plain per-expression kernel")
     ap.add_argument("--exprs", type=int, default=0,
@@ -312,6 +316,61 @@ def adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args):
     return res
 
 
+def cache_figures(ev, rank, flush_buf, sr_stream, args):
+    """Subtree-cache workload (4,096 expressions derived from 256 parents, 9
+    variables, 1M datapoints): one generation with the cross-generation cache
+    cleared (detect, fill the new subtrees, evaluate the skeletons) against
+    the same population without the cache."""
+    import torch
+    w = make_workload("cache", rank)
+    pop = w.population
+    node_evals = pop.num_tokens * w.num_dps
+    steps = max(3, min(args.steps, 5))
+    ev.set_data(w.X)
+    ev.prepare(pop)
+    _timed_launches(ev, torch, flush_buf, sr_stream, 1)
+    plain_ms = statistics.mean(_timed_launches(ev, torch, flush_buf, sr_stream, steps))
+    ev.prepare(pop, cache=True, clear_cache=True)
+    _timed_launches(ev, torch, flush_buf, sr_stream, 1)
+    cache_ms = statistics.mean(_timed_launches(ev, torch, flush_buf, sr_stream, steps))
+    ev.read_mse()
+    st = ev.stats
+    executed = int(st.node_evals_executed)
+    return {"workload": "cache", "exprs": pop.num_exprs, "num_dps": w.num_dps,
+            "num_vars": w.num_vars, "no_cache": {"value": node_evals / (plain_ms * 1e-3),
+                                                 "unit": UNIT, "ms": plain_ms},
+            "cached": {"value": node_evals / (cache_ms * 1e-3), "unit": UNIT, "ms": cache_ms,
+                       "executed_node_evals_per_s": executed / (cache_ms * 1e-3)},
+            "speedup": plain_ms / cache_ms, "num_subtrees": int(st.num_subtrees),
+            "new_subtrees": int(st.new_subtrees), "coverage": float(st.coverage),
+            "node_evals": int(node_evals), "node_evals_executed": executed,
+            "node_evals_saved": int(node_evals) - executed}
+
+
+def large_figures(ev, rank, flush_buf, sr_stream):
+    """The large population (100,000 expressions of 3-127 tokens, 0-8
+    constants, 10 variables, 4M datapoints): forward, fused forward+adjoint
+    and the plain per-expression kernel, one timed launch each after a
+    warm-up launch."""
+    import torch
+    from symbolic_regression_gpu_b200 import _lib
+    w = make_workload("large", rank)
+    pop = w.population
+    node_evals = pop.num_tokens * w.num_dps
+    ev.set_data(w.X)
+    res = {"workload": "large", "exprs": pop.num_exprs, "num_dps": w.num_dps,
+           "num_vars": w.num_vars, "tokens": int(pop.num_tokens)}
+    for name, kw in (("fwd", {}),
+                     ("fwd_adjoint", {"gradient": True, "grad_mode": _lib.SR_GRAD_CHECKPOINT}),
+                     ("plain_kernel", {"plain": True})):
+        ev.prepare(pop, **kw)
+        ms = _timed_launches(ev, torch, flush_buf, sr_stream, 2)[-1]
+        res[name] = {"value": node_evals / (ms * 1e-3), "unit": UNIT, "ms": ms}
+    res["fwd_adjoint"]["cost_vs_fwd"] = res["fwd_adjoint"]["ms"] / res["fwd"]["ms"]
+    res["fwd"]["vs_plain_kernel"] = res["plain_kernel"]["ms"] / res["fwd"]["ms"]
+    return res
+
+
 def run_ours(args):
     import torch
     rank, local_rank, world = dist_env()
@@ -413,6 +472,14 @@ def run_ours(args):
     if not args.no_adjoint:
         adjoint = adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args)
 
+    cache = None
+    if not args.no_cache_figures:
+        cache = cache_figures(ev, rank, flush_buf, sr_stream, args)
+    large = None
+    if args.large:
+        large = large_figures(ev, rank, flush_buf, sr_stream)
+        ev.set_data(w.X)
+
     # End to end through the public API: pinned host dataset and host
     # population in, MSE vector out, every step.
     Xp = torch.empty(w.X.shape, dtype=torch.float32, pin_memory=True)
@@ -476,6 +543,8 @@ def run_ours(args):
             "clocks": clk,
             "plain_kernel": plain,
             "fwd_adjoint": adjoint,
+            "subtree_cache": cache,
+            "large": large,
             "mse_finite": int(np.isfinite(mse).sum()),
         }
         print(json.dumps(line))
