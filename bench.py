@@ -50,6 +50,8 @@ def parse_args():
                     help="skip the forward+adjoint figures")
     ap.add_argument("--no-cache-figures", action="store_true",
                     help="skip the subtree-cache figures")
+    ap.add_argument("--no-evolution", action="store_true",
+                    help="skip the device generation-loop figures")
     ap.add_argument("--large", action="store_true",
                     help="also run the 100,000 x 4M population (about two minutes)")
     ap.add_argument("--plain-baseline", action="store_true",
@@ -347,6 +349,54 @@ def cache_figures(ev, rank, flush_buf, sr_stream, args):
             "node_evals_saved": int(node_evals) - executed}
 
 
+def evolution_figures(ev, w, torch, sr_stream, generations=5):
+    """The generation loop on the device on the batched dataset: a random
+    population of the same size, then per generation the device compile +
+    interpreter evaluation and the breeding step, device-timed."""
+    import ctypes
+
+    from symbolic_regression_gpu_b200 import _lib
+    from symbolic_regression_gpu_b200.evolution import DeviceEvolution
+    E = w.population.num_exprs
+    ev.set_data(w.X)
+    de = DeviceEvolution(ev, E, seed=2024)
+    de.init()
+    t_prep, t_eval, t_step, best = [], [], [], []
+    for g in range(generations + 1):
+        t0 = time.perf_counter()
+        t, v, n = de._bufs[de.cur]
+        ev._check(_lib.lib.sr_prepare_device_population(ev._ctx, ctypes.c_void_p(t.data_ptr()),
+                                                         ctypes.c_void_p(v.data_ptr()),
+                                                         ctypes.c_void_p(n.data_ptr()), E,
+                                                         de.stride),
+                   "sr_prepare_device_population")
+        t_prep.append((time.perf_counter() - t0) * 1e3)
+        ev._E = E
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(sr_stream)
+        ev.launch()
+        s1.record(sr_stream)
+        de._evaluated = True
+        mse = ev.read_mse()
+        t_eval.append(s0.elapsed_time(s1))
+        fin = mse[np.isfinite(mse)]
+        best.append(float(fin.min()) if fin.size else float("nan"))
+        if g == generations:
+            break
+        s2 = torch.cuda.Event(enable_timing=True)
+        s1.record(sr_stream)
+        de.step()
+        s2.record(sr_stream)
+        s2.synchronize()
+        t_step.append(s1.elapsed_time(s2))
+    ev.synchronize()
+    return {"exprs": E, "num_dps": w.num_dps, "generations": generations,
+            "prepare_ms_mean": statistics.mean(t_prep[1:]),
+            "eval_ms_mean": statistics.mean(t_eval[1:]),
+            "breed_ms_mean": statistics.mean(t_step[1:]) if len(t_step) > 1 else t_step[0],
+            "best_mse": best}
+
+
 def large_figures(ev, rank, flush_buf, sr_stream):
     """The large population (100,000 expressions of 3-127 tokens, 0-8
     constants, 10 variables, 4M datapoints): forward, fused forward+adjoint
@@ -475,6 +525,9 @@ def run_ours(args):
     cache = None
     if not args.no_cache_figures:
         cache = cache_figures(ev, rank, flush_buf, sr_stream, args)
+    evolution = None
+    if not args.no_evolution:
+        evolution = evolution_figures(ev, w, torch, sr_stream)
     large = None
     if args.large:
         large = large_figures(ev, rank, flush_buf, sr_stream)
@@ -544,6 +597,7 @@ def run_ours(args):
             "plain_kernel": plain,
             "fwd_adjoint": adjoint,
             "subtree_cache": cache,
+            "device_evolution": evolution,
             "large": large,
             "mse_finite": int(np.isfinite(mse).sum()),
         }

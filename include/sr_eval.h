@@ -348,6 +348,63 @@ sr_status sr_eval_mse_device_noalloc(const int32_t *tokens, const float *values,
                                      float *mse_out, void *stream);
 
 /* ---- misc ------------------------------------------------------------------ */
+/* ---- the generation loop on the device ---------------------------------------
+ * The reference runs its evolution loop on the host (src/cleaned/cl_sr_system.cpp:
+ * 150-330: evaluate, sort by fitness with NaN last, keep the top 5 %, fill the rest
+ * by size-3 tournaments with 20 % subtree mutation / 80 % subtree crossover,
+ * utils.cpp:1163-1273), packing every generation into InputInfo for the
+ * evaluator.  These calls run the same steps on the device, on a population held
+ * in device memory in a slot layout: expression i has lengths[i] tokens at
+ * tokens[i * stride ...] (int32) with values at values[i * stride ...] (float).
+ * Every call is enqueued on the context stream.  Random numbers come from a
+ * counter-based stream per (seed, generation, child): results are deterministic
+ * for a seed, with the reference's distributions but not its samples. */
+#define SR_EVOLVE_MAX_STRIDE 256
+typedef struct sr_evolve_options {
+  int32_t num_vars;       /* variables of generated leaves (EvolutionParams.num_vars) */
+  int32_t max_tokens;     /* 64 (EvolutionParams.max_tokens = MAX_TOKEN_NUM)          */
+  int32_t max_depth;      /* 5                                                         */
+  int32_t tournament;     /* 3 (cl_sr_system.cpp:301)                                  */
+  float const_min;        /* -5                                                        */
+  float const_max;        /* 5                                                         */
+  float prob_leaf;        /* 0.1                                                       */
+  float prob_const_leaf;  /* 0.5                                                       */
+  float prob_unary;       /* 0.35                                                      */
+  float elite_frac;       /* 0.05: elites = max(1, (int)(num_exprs * elite_frac))     */
+  float mutation_prob;    /* 0.2 (the rest is crossover)                               */
+  int32_t n_unary;        /* operator tables (reference kUnaryOps / kBinaryOps,        */
+  int32_t n_binary;       /*  utils.cpp:939-948: tokens 10..27 and 1..9)               */
+  int32_t unary_ops[32];
+  int32_t binary_ops[16];
+  uint64_t seed;
+} sr_evolve_options;
+/* The reference's parameters for `num_vars` input variables. */
+sr_status sr_evolve_options_init(sr_evolve_options *opts, int32_t num_vars);
+/* Generation 0: one random expression per slot (reference
+ * generate_random_expression, utils.cpp:1156-1161).  stride in
+ * [max_tokens, SR_EVOLVE_MAX_STRIDE]; 2 * max_tokens + 2 leaves room for the
+ * generator's budget-exhausted leaves (utils.cpp:1072-1078), below that a
+ * child that does not fit keeps its parent. */
+sr_status sr_evolve_init(sr_context *ctx, const sr_evolve_options *opts, int32_t num_exprs,
+                         int32_t stride, int32_t *tokens, float *values, int32_t *lengths);
+/* One breeding step from device fitness (for instance sr_device_mse after an
+ * evaluation on the same context).  The *_out buffers must not overlap the
+ * inputs. */
+sr_status sr_evolve_step(sr_context *ctx, const sr_evolve_options *opts, int32_t generation,
+                         int32_t num_exprs, int32_t stride, const float *fitness,
+                         const int32_t *tokens, const float *values, const int32_t *lengths,
+                         int32_t *tokens_out, float *values_out, int32_t *lengths_out);
+/* sr_prepare for a device-resident population in the slot layout: the
+ * programs are compiled on the device (the same bytecode the host compiler
+ * emits; constants and variable indices read from the float values), then
+ * sr_launch / sr_read_mse / sr_device_mse work as after sr_prepare.  Waits
+ * for the compile (one small device-to-host read: the spill-slot count and
+ * the validity flag); an invalid expression fails with
+ * SR_ERR_MALFORMED_EXPRESSION. */
+sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
+                                       const float *values, const int32_t *lengths,
+                                       int32_t num_exprs, int32_t stride);
+
 sr_status sr_get_stream(sr_context *ctx, void **stream);
 sr_status sr_synchronize(sr_context *ctx);
 /* Measured per-SM pipe peaks on this device (FP32 FMA lanes/clock and MUFU

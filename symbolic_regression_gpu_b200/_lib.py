@@ -125,6 +125,30 @@ class sr_adam_options(Structure):
     ]
 
 
+SR_EVOLVE_MAX_STRIDE = 256
+
+
+class sr_evolve_options(Structure):
+    _fields_ = [
+        ("num_vars", c_int32),
+        ("max_tokens", c_int32),
+        ("max_depth", c_int32),
+        ("tournament", c_int32),
+        ("const_min", c_float),
+        ("const_max", c_float),
+        ("prob_leaf", c_float),
+        ("prob_const_leaf", c_float),
+        ("prob_unary", c_float),
+        ("elite_frac", c_float),
+        ("mutation_prob", c_float),
+        ("n_unary", c_int32),
+        ("n_binary", c_int32),
+        ("unary_ops", c_int32 * 32),
+        ("binary_ops", c_int32 * 16),
+        ("seed", c_uint64),
+    ]
+
+
 # Every symbol the header declares, with its ctypes signature.
 _P = POINTER
 _SIGNATURES = {
@@ -163,6 +187,14 @@ _SIGNATURES = {
                                         _P(c_int64), _P(c_int32)]),
     "sr_eval_mse_device_noalloc": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                              c_int64, c_int32, c_int64, c_void_p, c_void_p]),
+    "sr_evolve_options_init": (c_int32, [_P(sr_evolve_options), c_int32]),
+    "sr_evolve_init": (c_int32, [c_void_p, _P(sr_evolve_options), c_int32, c_int32, c_void_p,
+                                 c_void_p, c_void_p]),
+    "sr_evolve_step": (c_int32, [c_void_p, _P(sr_evolve_options), c_int32, c_int32, c_int32,
+                                 c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p]),
+    "sr_prepare_device_population": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
+                                               c_int32]),
     "sr_get_stream": (c_int32, [c_void_p, _P(c_void_p)]),
     "sr_synchronize": (c_int32, [c_void_p]),
     "sr_measure_pipes": (c_int32, [c_void_p, _P(c_double), _P(c_double), _P(c_int32)]),

@@ -21,6 +21,7 @@
 
 #include "sr_adjoint.hpp"
 #include "sr_context.hpp"
+#include "sr_evolve.hpp"
 #include "sr_kernels.hpp"
 
 using sr::Instr;
@@ -1368,6 +1369,202 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
     fill_stats(ctx, stats);
     stats->total_eval_time_ms = now_ms() - t0;
   }
+  return SR_OK;
+}
+
+// ---- the generation loop on the device ------------------------------------------
+
+sr_status sr_evolve_options_init(sr_evolve_options *o, int32_t num_vars) {
+  if (!o) return SR_ERR_INVALID_ARGUMENT;
+  *o = sr_evolve_options{};
+  // Reference EvolutionParams defaults (src/utils/utils.h:178-187) and loop
+  // constants (src/cleaned/cl_sr_system.cpp:293-309).
+  o->num_vars = num_vars;
+  o->max_tokens = 64;
+  o->max_depth = 5;
+  o->tournament = 3;
+  o->const_min = -5.0f;
+  o->const_max = 5.0f;
+  o->prob_leaf = 0.1f;
+  o->prob_const_leaf = 0.5f;
+  o->prob_unary = 0.35f;
+  o->elite_frac = 0.05f;
+  o->mutation_prob = 0.2f;
+  o->n_unary = 18;  // SIN .. LOOSE_SQRT (utils.cpp:939-943)
+  for (int k = 0; k < 18; ++k) o->unary_ops[k] = 10 + k;
+  o->n_binary = 9;  // ADD .. LOOSE_POW (utils.cpp:945-948)
+  for (int k = 0; k < 9; ++k) o->binary_ops[k] = 1 + k;
+  o->seed = 0x5EED5EEDull;
+  return SR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+sr_status evolve_params(sr_context *ctx, const sr_evolve_options *o, int E, int stride,
+                        sr::EvolveParams *p) {
+  if (!o) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "evolve options are NULL");
+  if (E < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "negative population size");
+  if (o->num_vars < 0 || o->num_vars > SR_MAX_VARS)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "num_vars out of range");
+  if (o->max_tokens < 1 || o->max_depth < 0 || o->max_depth > 62 || o->tournament < 1)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad max_tokens / max_depth / tournament");
+  if (stride < o->max_tokens || stride > SR_EVOLVE_MAX_STRIDE)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT,
+                     "stride must lie in [max_tokens, " + std::to_string(SR_EVOLVE_MAX_STRIDE) +
+                         "]");
+  if (o->n_unary < 1 || o->n_unary > 32 || o->n_binary < 1 || o->n_binary > 16)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "operator tables must be non-empty");
+  for (int k = 0; k < o->n_unary; ++k)
+    if (!sr::is_unary_token(o->unary_ops[k]))
+      return ctx->fail(SR_ERR_BAD_TOKEN, "unary_ops[" + std::to_string(k) + "] is not unary");
+  for (int k = 0; k < o->n_binary; ++k)
+    if (!sr::is_binary_token(o->binary_ops[k]))
+      return ctx->fail(SR_ERR_BAD_TOKEN, "binary_ops[" + std::to_string(k) + "] is not binary");
+  const float probs[] = {o->prob_leaf, o->prob_const_leaf, o->prob_unary, o->elite_frac,
+                         o->mutation_prob};
+  for (float q : probs)
+    if (!(q >= 0.0f && q <= 1.0f)) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "probability outside [0, 1]");
+  if (!(o->const_min <= o->const_max)) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "const_min > const_max");
+  sr::EvolveParams q{};
+  q.num_vars = o->num_vars;
+  q.max_tokens = o->max_tokens;
+  q.max_depth = o->max_depth;
+  q.tournament = o->tournament;
+  q.const_min = o->const_min;
+  q.const_max = o->const_max;
+  q.prob_leaf = o->prob_leaf;
+  q.prob_const_leaf = o->prob_const_leaf;
+  q.prob_unary = o->prob_unary;
+  q.mutation_prob = o->mutation_prob;
+  q.n_unary = o->n_unary;
+  q.n_binary = o->n_binary;
+  std::memcpy(q.unary_ops, o->unary_ops, sizeof q.unary_ops);
+  std::memcpy(q.binary_ops, o->binary_ops, sizeof q.binary_ops);
+  q.seed = o->seed;
+  *p = q;
+  return SR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sr_status sr_evolve_init(sr_context *ctx, const sr_evolve_options *opts, int32_t num_exprs,
+                         int32_t stride, int32_t *tokens, float *values, int32_t *lengths) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  sr::EvolveParams p;
+  SR_TRY(evolve_params(ctx, opts, num_exprs, stride, &p));
+  if (num_exprs == 0) return SR_OK;
+  if (!tokens || !values || !lengths) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL buffer");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, sr::launch_evolve_init(p, num_exprs, stride, tokens, values, lengths,
+                                          ctx->stream));
+  return SR_OK;
+}
+
+sr_status sr_evolve_step(sr_context *ctx, const sr_evolve_options *opts, int32_t generation,
+                         int32_t num_exprs, int32_t stride, const float *fitness,
+                         const int32_t *tokens, const float *values, const int32_t *lengths,
+                         int32_t *tokens_out, float *values_out, int32_t *lengths_out) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  sr::EvolveParams p;
+  SR_TRY(evolve_params(ctx, opts, num_exprs, stride, &p));
+  const int E = num_exprs;
+  if (E == 0) return SR_OK;
+  if (!fitness || !tokens || !values || !lengths || !tokens_out || !values_out || !lengths_out)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL buffer");
+  const size_t slots = static_cast<size_t>(E) * static_cast<size_t>(stride);
+  auto overlaps = [&](const void *a, const void *b, size_t bytes) {
+    const char *x = static_cast<const char *>(a), *y = static_cast<const char *>(b);
+    return x < y + bytes && y < x + bytes;
+  };
+  if (overlaps(tokens, tokens_out, slots * sizeof(int32_t)) ||
+      overlaps(values, values_out, slots * sizeof(float)) ||
+      overlaps(lengths, lengths_out, static_cast<size_t>(E) * sizeof(int32_t)))
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "output buffers overlap the inputs");
+  DeviceScope scope(ctx->device);
+  const size_t temp = sr::rank_temp_bytes(E);
+  const bool grow = ctx->evo_temp.cap < std::max<size_t>(temp, 1) ||
+                    ctx->evo_keys.cap < 2 * static_cast<size_t>(E) ||
+                    ctx->evo_order.cap < static_cast<size_t>(E);
+  if (grow) SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  SR_TRY_CUDA(ctx, ctx->evo_temp.ensure(std::max<size_t>(temp, 1)));
+  SR_TRY_CUDA(ctx, ctx->evo_keys.ensure(2 * static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->evo_idx.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->evo_order.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->evo_fit.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, sr::launch_rank(fitness, E, ctx->evo_temp.p, ctx->evo_temp.cap,
+                                   ctx->evo_keys.p, ctx->evo_idx.p, ctx->evo_order.p,
+                                   ctx->evo_fit.p, ctx->stream));
+  int elites = static_cast<int>(static_cast<double>(E) * static_cast<double>(opts->elite_frac));
+  elites = std::min(std::max(elites, 1), E);
+  SR_TRY_CUDA(ctx, sr::launch_evolve_step(p, generation, E, stride, elites, ctx->evo_order.p,
+                                          ctx->evo_fit.p, tokens, values, lengths, tokens_out,
+                                          values_out, lengths_out, ctx->stream));
+  return SR_OK;
+}
+
+sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
+                                       const float *values, const int32_t *lengths,
+                                       int32_t num_exprs, int32_t stride) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  if (num_exprs < 0 || stride < 1 || stride > SR_EVOLVE_MAX_STRIDE)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad population size or stride");
+  if (num_exprs > 0 && (!tokens || !values || !lengths))
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL buffer");
+  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  reset_prepared(ctx);
+  ctx->prep_stats = sr_stats{};
+  const int E = num_exprs;
+  ctx->E = E;
+  if (E == 0) return SR_OK;
+  const double t0 = now_ms();
+  ProgramSet &ps = ctx->main;
+  ps.E = E;
+  const size_t n_code = static_cast<size_t>(E) * (static_cast<size_t>(stride) + 1) + 1;
+  SR_TRY_CUDA(ctx, ps.code.ensure(n_code));
+  SR_TRY_CUDA(ctx, ps.off.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ps.len.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->evo_summary.ensure(6));
+  SR_TRY_CUDA(ctx, ctx->h_evo_summary.ensure(6));
+  SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
+  // The interpreter prefetches one instruction past a program: keep the
+  // padding word defined.
+  SR_TRY_CUDA(ctx, cudaMemsetAsync(ps.code.p + (n_code - 1), 0, sizeof(Instr), ctx->stream));
+  SR_TRY_CUDA(ctx, sr::launch_compile_device(tokens, values, lengths, E, stride, ctx->V,
+                                             ps.code.p, ps.off.p, ps.len.p, ctx->evo_summary.p,
+                                             ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_evo_summary.p, ctx->evo_summary.p, 6 * sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int32_t *sm = ctx->h_evo_summary.p;
+  if (sm[1] != 0)
+    return ctx->fail(SR_ERR_MALFORMED_EXPRESSION,
+                     "the device population holds an invalid expression (or one longer than "
+                     "the stride)");
+  int64_t n_tok = 0, n_ins = 0;
+  std::memcpy(&n_tok, sm + 2, sizeof n_tok);
+  std::memcpy(&n_ins, sm + 4, sizeof n_ins);
+  ps.smax = sm[0];
+  ps.n_tokens = n_tok;
+  ps.n_instr = n_ins;
+  ps.cost.assign(static_cast<size_t>(E), 0.0f);  // groups in population order
+  ps.n_const.assign(static_cast<size_t>(E), 0);
+  ps.sfu_per_dp = 0.0;
+  ps.fp32_per_dp = 0.0;
+  ctx->prep_stats.host_compile_time_ms = now_ms() - t0;
+  SR_TRY(prepare_main_shape(ctx, false));
+  ctx->prep_stats.node_evals = n_tok * ctx->N;
+  ctx->prep_stats.node_evals_executed = ctx->prep_stats.node_evals;
+  ctx->mode = sr::Mode::kBatched;
   return SR_OK;
 }
 

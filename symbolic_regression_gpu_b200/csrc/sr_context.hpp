@@ -206,6 +206,14 @@ struct sr_context {
   sr::DevBuf<float> spill;
   // gradients / constant optimisation
   sr::GradSet grad;
+  // device-side evolution: ranking scratch and the device-compile summary
+  sr::DevBuf<unsigned char> evo_temp;
+  sr::DevBuf<uint32_t> evo_keys;   // [2E]
+  sr::DevBuf<int32_t> evo_idx;     // [E]
+  sr::DevBuf<int32_t> evo_order;   // [E]
+  sr::DevBuf<float> evo_fit;       // [E] fitness in rank order
+  sr::DevBuf<int32_t> evo_summary; // [6] see launch_compile_device
+  sr::PinnedBuf<int32_t> h_evo_summary;
 
   // timing
   cudaEvent_t ev[6] = {};

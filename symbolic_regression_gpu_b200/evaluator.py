@@ -38,6 +38,7 @@ class Evaluator:
                  tune_cache_path: Optional[str] = None, stream=None, use_graphs: bool = False):
         opts = _lib.sr_options()
         _lib.check(_lib.lib.sr_options_init(ctypes.byref(opts)))
+        self.device = device
         opts.device = device
         opts.cache_capacity = cache_capacity
         opts.min_subtree_size = min_subtree_size
