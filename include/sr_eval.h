@@ -405,6 +405,29 @@ sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
                                        const float *values, const int32_t *lengths,
                                        int32_t num_exprs, int32_t stride);
 
+/* ---- file loaders (host, no device needed) ------------------------------------
+ * Parallel readers of the reference's text files: the file is memory-mapped,
+ * cut into line-aligned chunks and parsed by `threads` host threads (0 = all
+ * cores).  Numbers are parsed correctly rounded (as strtod) into doubles;
+ * dataset values are narrowed to float exactly like the reference loop
+ * (cl_sr_system.cpp:98-104).  Unlike the reference's stream readers they
+ * expect the files' line structure: one datapoint per line, four lines per
+ * expression.  Call with the output pointers NULL to get the sizes first. */
+/* shared_data.txt (reference load_data_file, utils.cpp:235-300): X[v * ld + j]
+ * = column v (x0 .. x_{num_vars-1}, y) of datapoint j, for the first
+ * min(lines, max_dps) datapoints (max_dps < 0: all); *num_dps receives that
+ * count.  SR_ERR_MALFORMED_EXPRESSION if a line does not hold num_vars + 1
+ * numbers. */
+sr_status sr_load_shared_data(const char *path, int32_t num_vars, int64_t max_dps, float *X,
+                              int64_t ld, int64_t *num_dps, int32_t threads);
+/* gen_N.txt (reference parse_input_info, utils.cpp:122-233): the population in
+ * CSR form (offsets[num_exprs + 1]), each expression's num_vars / num_dps
+ * (nullable) and the first expression's data file name (nullable). */
+sr_status sr_load_population(const char *path, int32_t *num_exprs, int64_t *num_tokens,
+                             int32_t *tokens, double *values, int64_t *offsets,
+                             int32_t *num_vars, int32_t *num_dps, char *data_file,
+                             int32_t data_file_cap, int32_t threads);
+
 sr_status sr_get_stream(sr_context *ctx, void **stream);
 sr_status sr_synchronize(sr_context *ctx);
 /* Measured per-SM pipe peaks on this device (FP32 FMA lanes/clock and MUFU

@@ -195,6 +195,11 @@ _SIGNATURES = {
                                  c_void_p]),
     "sr_prepare_device_population": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                                                c_int32]),
+    "sr_load_shared_data": (c_int32, [c_char_p, c_int32, c_int64, _P(c_float), c_int64,
+                                      _P(c_int64), c_int32]),
+    "sr_load_population": (c_int32, [c_char_p, _P(c_int32), _P(c_int64), _P(c_int32),
+                                     _P(c_double), _P(c_int64), _P(c_int32), _P(c_int32),
+                                     c_char_p, c_int32, c_int32]),
     "sr_get_stream": (c_int32, [c_void_p, _P(c_void_p)]),
     "sr_synchronize": (c_int32, [c_void_p]),
     "sr_measure_pipes": (c_int32, [c_void_p, _P(c_double), _P(c_double), _P(c_int32)]),
