@@ -338,6 +338,15 @@ def cache_figures(ev, rank, flush_buf, sr_stream, args):
     ev.read_mse()
     st = ev.stats
     executed = int(st.node_evals_executed)
+    # common-subtree detection alone: host detector vs the device one
+    from symbolic_regression_gpu_b200.evaluator import detect_subtrees
+    detect_subtrees(pop, evaluator=ev)  # warm-up (buffers, cub)
+    t0 = time.perf_counter()
+    detect_subtrees(pop)
+    t_host = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    detect_subtrees(pop, evaluator=ev)
+    t_dev = (time.perf_counter() - t0) * 1e3
     return {"workload": "cache", "exprs": pop.num_exprs, "num_dps": w.num_dps,
             "num_vars": w.num_vars, "no_cache": {"value": node_evals / (plain_ms * 1e-3),
                                                  "unit": UNIT, "ms": plain_ms},
@@ -346,7 +355,9 @@ def cache_figures(ev, rank, flush_buf, sr_stream, args):
             "speedup": plain_ms / cache_ms, "num_subtrees": int(st.num_subtrees),
             "new_subtrees": int(st.new_subtrees), "coverage": float(st.coverage),
             "node_evals": int(node_evals), "node_evals_executed": executed,
-            "node_evals_saved": int(node_evals) - executed}
+            "node_evals_saved": int(node_evals) - executed,
+            "detect_ms": {"host": t_host, "device": t_dev,
+                          "host_threads": os.cpu_count() or 1}}
 
 
 def evolution_figures(ev, w, torch, sr_stream, generations=5):

@@ -122,7 +122,8 @@ typedef struct sr_options {
                                a CUDA graph on first use and replays it until
                                the next sr_prepare / sr_set_data            */
   int32_t host_threads;     /* host compile threads; 0 = hardware concurrency  */
-  int32_t reserved0;
+  int32_t device_detect;    /* 1 = the subtree-cache path detects common
+                               subtrees on the device (same result)           */
   const char *tune_cache_path; /* JSON file for tuned shapes; NULL = none      */
   void *stream;             /* cudaStream_t to run on; NULL = own stream      */
 } sr_options;
@@ -288,6 +289,15 @@ sr_status sr_detect_subtrees(const sr_population *pop, int32_t min_size, int32_t
                              int32_t max_groups, sr_detect_result *res, int32_t *group_expr,
                              int32_t *group_pos, int32_t *group_size, int32_t *group_count,
                              uint64_t *group_key);
+
+/* The same detection on the context's GPU (csrc/sr_detect_gpu.cu): Merkle
+ * hashes per expression, candidates sorted and grouped by hash, groups
+ * verified member by member, cover counted per expression; identical
+ * groups, order and statistics.  Synchronous. */
+sr_status sr_detect_subtrees_device(sr_context *ctx, const sr_population *pop, int32_t min_size,
+                                    int32_t min_freq, int32_t max_groups, sr_detect_result *res,
+                                    int32_t *group_expr, int32_t *group_pos, int32_t *group_size,
+                                    int32_t *group_count, uint64_t *group_key);
 
 /* Cache marking (reference mark_cached_subtrees_from_state,
  * src/cleaned/cl_gpu_eval.cu:294-329): given cached keys and their slots,

@@ -57,7 +57,7 @@ class sr_options(Structure):
         ("autotune", c_int32),
         ("use_graphs", c_int32),
         ("host_threads", c_int32),
-        ("reserved0", c_int32),
+        ("device_detect", c_int32),
         ("tune_cache_path", c_char_p),
         ("stream", c_void_p),
     ]
@@ -179,6 +179,9 @@ _SIGNATURES = {
     "sr_detect_subtrees": (c_int32, [_P(sr_population), c_int32, c_int32, c_int32,
                                      _P(sr_detect_result), _P(c_int32), _P(c_int32), _P(c_int32),
                                      _P(c_int32), _P(c_uint64)]),
+    "sr_detect_subtrees_device": (c_int32, [c_void_p, _P(sr_population), c_int32, c_int32,
+                                            c_int32, _P(sr_detect_result), _P(c_int32),
+                                            _P(c_int32), _P(c_int32), _P(c_int32), _P(c_uint64)]),
     "sr_mark_cached": (c_int32, [_P(sr_population), _P(c_uint64), _P(c_int32), c_int32,
                                  _P(c_int32)]),
     "sr_validate_population": (c_int32, [_P(sr_population), c_int32, _P(c_int32), _P(c_int32),

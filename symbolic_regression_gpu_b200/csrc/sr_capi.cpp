@@ -21,6 +21,7 @@
 
 #include "sr_adjoint.hpp"
 #include "sr_context.hpp"
+#include "sr_detect_gpu.hpp"
 #include "sr_evolve.hpp"
 #include "sr_kernels.hpp"
 
@@ -658,6 +659,116 @@ static sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
   return SR_OK;
 }
 
+// Common-subtree detection on the context's GPU: the same Detection as
+// sr::detect_common_subtrees (groups largest first, stable in hash order).
+static sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, const double *val,
+                                  const int64_t *off, int min_size, int min_freq,
+                                  sr::Detection &out) {
+  out = sr::Detection{};
+  out.total_tokens = E > 0 ? off[E] - off[0] : 0;
+  const int64_t T = out.total_tokens;
+  if (E <= 0 || T <= 0) return SR_OK;
+  if (T >= (1ll << 31)) return ctx->fail(SR_ERR_UNSUPPORTED, "population too large for device detection");
+  sr::DetectBufs &b = ctx->det;
+  cudaStream_t s = ctx->stream;
+  const size_t n = static_cast<size_t>(T);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(s));  // buffers may grow
+  SR_TRY_CUDA(ctx, b.tok.ensure(n));
+  SR_TRY_CUDA(ctx, b.val.ensure(n));
+  SR_TRY_CUDA(ctx, b.off.ensure(static_cast<size_t>(E) + 1));
+  for (auto *buf : {&b.size, &b.pos_in, &b.pos_out, &b.run_count, &b.run_start, &b.rep, &b.gsize,
+                    &b.vcount})
+    SR_TRY_CUDA(ctx, buf->ensure(n));
+  SR_TRY_CUDA(ctx, b.out3.ensure(3 * n));
+  for (auto *buf : {&b.hash, &b.key_in, &b.key_out, &b.run_key}) SR_TRY_CUDA(ctx, buf->ensure(n));
+  SR_TRY_CUDA(ctx, b.cand.ensure(n));
+  SR_TRY_CUDA(ctx, b.mark.ensure(n));
+  SR_TRY_CUDA(ctx, b.counters.ensure(2));
+  SR_TRY_CUDA(ctx, b.covered.ensure(1));
+  SR_TRY_CUDA(ctx, b.h_counters.ensure(2));
+  SR_TRY_CUDA(ctx, b.h_covered.ensure(1));
+  const size_t temp = std::max(sr::detect_scratch_sizes(T).temp_bytes,
+                               sr::detect_scan_temp_bytes(static_cast<int>(T)));
+  SR_TRY_CUDA(ctx, b.temp.ensure(std::max<size_t>(temp, 1)));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(b.tok.p, tok + off[0], n * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, s));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(b.val.p, val + off[0], n * sizeof(double),
+                                   cudaMemcpyHostToDevice, s));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(b.off.p, off, (static_cast<size_t>(E) + 1) * sizeof(int64_t),
+                                   cudaMemcpyHostToDevice, s));
+  sr::DetectArgs a{};
+  a.tok = b.tok.p;
+  a.val = b.val.p;
+  a.off = b.off.p;
+  a.E = E;
+  a.T = T;
+  a.min_size = min_size;
+  a.min_freq = min_freq;
+  a.size = b.size.p;
+  a.hash = b.hash.p;
+  a.cand = b.cand.p;
+  a.mark = b.mark.p;
+  a.pos_in = b.pos_in.p;
+  a.pos_out = b.pos_out.p;
+  a.key_in = b.key_in.p;
+  a.key_out = b.key_out.p;
+  a.run_key = b.run_key.p;
+  a.run_count = b.run_count.p;
+  a.run_start = b.run_start.p;
+  a.rep = b.rep.p;
+  a.gsize = b.gsize.p;
+  a.vcount = b.vcount.p;
+  a.n_sel = b.counters.p;
+  a.n_runs = b.counters.p + 1;
+  a.covered = b.covered.p;
+  a.temp = b.temp.p;
+  a.temp_bytes = b.temp.cap;
+  auto read_counters = [&]() -> sr_status {
+    SR_TRY_CUDA(ctx, cudaMemcpyAsync(b.h_counters.p, b.counters.p, 2 * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, s));
+    SR_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    return SR_OK;
+  };
+  SR_TRY_CUDA(ctx, cudaMemsetAsync(b.counters.p, 0, 2 * sizeof(int32_t), s));
+  SR_TRY_CUDA(ctx, sr::detect_candidates(a, s));
+  SR_TRY(read_counters());
+  const int M = b.h_counters.p[0];
+  SR_TRY_CUDA(ctx, sr::detect_groups(a, M, s));
+  SR_TRY(read_counters());
+  const int R = M > 0 ? b.h_counters.p[1] : 0;
+  SR_TRY_CUDA(ctx, sr::detect_verify(a, R, s));
+  SR_TRY_CUDA(ctx, sr::detect_frequent(a, R, b.out3.p, s));
+  SR_TRY(read_counters());
+  const int F = R > 0 ? b.h_counters.p[0] : 0;
+  SR_TRY_CUDA(ctx, b.h_out3.ensure(static_cast<size_t>(3 * std::max(F, 1))));
+  if (F > 0)
+    SR_TRY_CUDA(ctx, cudaMemcpyAsync(b.h_out3.p, b.out3.p, 3 * static_cast<size_t>(F) * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, s));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(b.h_covered.p, b.covered.p, sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, s));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+  // Groups in hash order -> size descending, stable.
+  std::vector<int> order(static_cast<size_t>(F));
+  std::iota(order.begin(), order.end(), 0);
+  const int32_t *o3 = b.h_out3.p;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return o3[3 * x + 1] > o3[3 * y + 1]; });
+  int64_t size_sum = 0;
+  out.groups.reserve(static_cast<size_t>(F));
+  for (int k : order) {
+    const int64_t g = o3[3 * k] + off[0];  // absolute token index
+    const int64_t *it = std::upper_bound(off, off + E + 1, g) - 1;
+    const int32_t x = static_cast<int32_t>(it - off);
+    out.groups.push_back(sr::Detection::Group{x, static_cast<int32_t>(g - off[x]), o3[3 * k + 1],
+                                              o3[3 * k + 2]});
+    size_sum += o3[3 * k + 1];
+  }
+  out.covered_tokens = static_cast<int64_t>(*b.h_covered.p);
+  out.avg_subtree_size = F > 0 ? static_cast<double>(size_sum) / F : 0.0;
+  out.coverage = T > 0 ? static_cast<double>(out.covered_tokens) / T : 0.0;
+  return SR_OK;
+}
+
 static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint32_t flags) {
   const int E = pop->num_exprs;
   const int64_t T = pop->offsets[E];
@@ -679,8 +790,13 @@ static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint3
   const int threads = host_threads(ctx);
   const double t0 = now_ms();
   sr::Detection det;
-  sr::detect_common_subtrees(E, pop->tokens, pop->values, pop->offsets,
-                             ctx->opts.min_subtree_size, ctx->opts.min_subtree_freq, threads, det);
+  if (ctx->opts.device_detect)
+    SR_TRY(detect_on_device(ctx, E, pop->tokens, pop->values, pop->offsets,
+                            ctx->opts.min_subtree_size, ctx->opts.min_subtree_freq, det));
+  else
+    sr::detect_common_subtrees(E, pop->tokens, pop->values, pop->offsets,
+                               ctx->opts.min_subtree_size, ctx->opts.min_subtree_freq, threads,
+                               det);
   ctx->prep_stats.detect_time_ms = now_ms() - t0;
   ctx->prep_stats.num_subtrees = static_cast<int32_t>(det.groups.size());
   ctx->prep_stats.avg_subtree_size = det.avg_subtree_size;
@@ -1641,6 +1757,39 @@ sr_status sr_detect_subtrees(const sr_population *pop, int32_t min_size, int32_t
   sr::Detection det;
   sr::detect_common_subtrees(pop->num_exprs, pop->tokens, pop->values, pop->offsets, min_size,
                              min_freq, static_cast<int>(std::thread::hardware_concurrency()), det);
+  res->num_subtrees = static_cast<int32_t>(det.groups.size());
+  res->total_tokens = det.total_tokens;
+  res->covered_tokens = det.covered_tokens;
+  res->avg_subtree_size = det.avg_subtree_size;
+  res->coverage = det.coverage;
+  const int n = std::min<int>(std::max(max_groups, 0), static_cast<int>(det.groups.size()));
+  for (int g = 0; g < n; ++g) {
+    const auto &G = det.groups[static_cast<size_t>(g)];
+    if (group_expr) group_expr[g] = G.expr;
+    if (group_pos) group_pos[g] = G.pos;
+    if (group_size) group_size[g] = G.size;
+    if (group_count) group_count[g] = G.occurrences;
+    if (group_key)
+      group_key[g] = sr::flat_key(pop->tokens + pop->offsets[G.expr] + G.pos,
+                                  pop->values + pop->offsets[G.expr] + G.pos, G.size);
+  }
+  return SR_OK;
+}
+
+sr_status sr_detect_subtrees_device(sr_context *ctx, const sr_population *pop, int32_t min_size,
+                                    int32_t min_freq, int32_t max_groups, sr_detect_result *res,
+                                    int32_t *group_expr, int32_t *group_pos, int32_t *group_size,
+                                    int32_t *group_count, uint64_t *group_key) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  if (!pop || !res || pop->num_exprs < 0 || min_size < 1 || min_freq < 1)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad detection arguments");
+  if (pop->num_exprs > 0 && (!pop->tokens || !pop->values || !pop->offsets))
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL population arrays");
+  DeviceScope scope(ctx->device);
+  sr::Detection det;
+  SR_TRY(detect_on_device(ctx, pop->num_exprs, pop->tokens, pop->values, pop->offsets, min_size,
+                          min_freq, det));
   res->num_subtrees = static_cast<int32_t>(det.groups.size());
   res->total_tokens = det.total_tokens;
   res->covered_tokens = det.covered_tokens;

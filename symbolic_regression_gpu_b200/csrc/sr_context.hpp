@@ -136,6 +136,23 @@ struct AdjClass {
   Plan plan;
 };
 
+// Buffers of the device common-subtree detection (sr_detect_gpu.cu), per
+// token of the population unless noted.
+struct DetectBufs {
+  DevBuf<int32_t> tok;
+  DevBuf<double> val;
+  DevBuf<int64_t> off;      // [E + 1]
+  DevBuf<int32_t> size, pos_in, pos_out, run_count, run_start, rep, gsize, vcount, out3;
+  DevBuf<uint64_t> hash, key_in, key_out, run_key;
+  DevBuf<uint8_t> cand, mark;
+  DevBuf<int32_t> counters;               // [2]: candidates, runs
+  DevBuf<unsigned long long> covered;     // [1]
+  DevBuf<unsigned char> temp;
+  PinnedBuf<int32_t> h_counters;
+  PinnedBuf<unsigned long long> h_covered;
+  PinnedBuf<int32_t> h_out3;
+};
+
 // Device state of a gradient / constant-optimisation call.
 struct GradSet {
   DevBuf<int64_t> const_off;
@@ -206,6 +223,8 @@ struct sr_context {
   sr::DevBuf<float> spill;
   // gradients / constant optimisation
   sr::GradSet grad;
+  // device common-subtree detection
+  sr::DetectBufs det;
   // device-side evolution: ranking scratch and the device-compile summary
   sr::DevBuf<unsigned char> evo_temp;
   sr::DevBuf<uint32_t> evo_keys;   // [2E]

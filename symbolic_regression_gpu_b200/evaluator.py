@@ -35,7 +35,8 @@ class Evaluator:
     def __init__(self, device: int = -1, *, cache_capacity: int = 2048,
                  min_subtree_size: int = 3, min_subtree_freq: int = 10, dpt: int = 0,
                  warps_per_block: int = 0, autotune: bool = False, host_threads: int = 0,
-                 tune_cache_path: Optional[str] = None, stream=None, use_graphs: bool = False):
+                 tune_cache_path: Optional[str] = None, stream=None, use_graphs: bool = False,
+                 device_detect: bool = False):
         opts = _lib.sr_options()
         _lib.check(_lib.lib.sr_options_init(ctypes.byref(opts)))
         self.device = device
@@ -47,6 +48,7 @@ class Evaluator:
         opts.warps_per_block = warps_per_block
         opts.autotune = 1 if autotune else 0
         opts.use_graphs = 1 if use_graphs else 0
+        opts.device_detect = 1 if device_detect else 0
         opts.host_threads = host_threads
         self._tune_path = tune_cache_path.encode() if tune_cache_path else None
         opts.tune_cache_path = self._tune_path
@@ -250,13 +252,24 @@ def subtree_hashes(tokens, values):
     return sizes, hashes
 
 
-def detect_subtrees(pop: Population, min_size: int = 3, min_freq: int = 10):
+def detect_subtrees(pop: Population, min_size: int = 3, min_freq: int = 10,
+                    evaluator: Optional["Evaluator"] = None):
     """Common-subtree detection (reference detect_common_subtrees,
-    src/utils/detect.cpp:120-387).  Returns (stats dict, groups dict of arrays)."""
+    src/utils/detect.cpp:120-387).  Returns (stats dict, groups dict of arrays).
+    With an ``evaluator`` the detection runs on its GPU
+    (sr_detect_subtrees_device), else on the host."""
     res = _lib.sr_detect_result()
     cpop = pop.as_c()
-    _lib.check(_lib.lib.sr_detect_subtrees(ctypes.byref(cpop), min_size, min_freq, 0,
-                                           ctypes.byref(res), None, None, None, None, None))
+    if evaluator is not None:
+        ctx = evaluator._ctx
+
+        def call(*a):
+            return _lib.lib.sr_detect_subtrees_device(ctx, *a)
+    else:
+        ctx = None
+        call = _lib.lib.sr_detect_subtrees
+    _lib.check(call(ctypes.byref(cpop), min_size, min_freq, 0, ctypes.byref(res), None, None,
+                    None, None, None), ctx)
     n = res.num_subtrees
     ge = np.empty(max(n, 1), np.int32)
     gp = np.empty(max(n, 1), np.int32)
@@ -264,11 +277,11 @@ def detect_subtrees(pop: Population, min_size: int = 3, min_freq: int = 10):
     gc = np.empty(max(n, 1), np.int32)
     gk = np.empty(max(n, 1), np.uint64)
     P = ctypes.POINTER
-    _lib.check(_lib.lib.sr_detect_subtrees(
+    _lib.check(call(
         ctypes.byref(cpop), min_size, min_freq, n, ctypes.byref(res),
         ge.ctypes.data_as(P(ctypes.c_int32)), gp.ctypes.data_as(P(ctypes.c_int32)),
         gs.ctypes.data_as(P(ctypes.c_int32)), gc.ctypes.data_as(P(ctypes.c_int32)),
-        gk.ctypes.data_as(P(ctypes.c_uint64))))
+        gk.ctypes.data_as(P(ctypes.c_uint64))), ctx)
     stats = {f: getattr(res, f) for f, _ in res._fields_ if f != "reserved0"}
     groups = {"expr": ge[:n], "pos": gp[:n], "size": gs[:n], "count": gc[:n], "key": gk[:n]}
     return stats, groups
