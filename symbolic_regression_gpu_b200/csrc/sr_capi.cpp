@@ -144,6 +144,10 @@ sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *
     pos += static_cast<int64_t>(c.size());
   }
   ps.h_code.p[total] = Instr{0, 0, 0, 0};  // prefetch padding
+  int64_t in_profile = 0;
+  for (int64_t i = 0; i < total; ++i)
+    in_profile += sr::in_protected_profile(sr::instr_op(ps.h_code.p[i].w)) ? 1 : 0;
+  ps.n_instr_protected = in_profile;
   int64_t o = 0;
   for (int x = 0; x < E; ++x) {
     const auto &in = infos[static_cast<size_t>(x)];
@@ -167,6 +171,10 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   sr::Plan p;
   p.dpt = dpt;
   p.W = W;
+  p.ops = (!pred && ps.n_instr > 0 &&
+           static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr)
+              ? sr::kOpsProtected
+              : sr::kOpsAll;
   p.smax = std::max(ps.smax, 0);
   p.s_smem = std::min(p.smax, sr::smem_spill_slots(dpt));
   const int64_t tile = 32 * dpt;
@@ -192,7 +200,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   if (!pred && static_cast<double>(p.n_spans) * E * 16.0 > 8.0 * (1ull << 30))
     return ctx->fail(SR_ERR_UNSUPPORTED, "partial-sum buffer would exceed 8 GiB");
   int bps = 0;
-  SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.smem, W, &bps));
+  SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.smem, W, &bps));
   if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
   const int64_t resident = static_cast<int64_t>(bps) * ctx->num_sms;
   p.blocks = static_cast<int>(std::min<int64_t>(resident, std::max<int64_t>(p.items(), 1)));
@@ -276,7 +284,7 @@ sr_status launch_set(sr_context *ctx, ProgramSet &ps, bool pred, int32_t *counte
   a.ldp = ldp;
   a.pred_row = pred_row;
   SR_TRY_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int32_t), ctx->stream));
-  SR_TRY_CUDA(ctx, sr::launch_interp(ps.plan.dpt, pred, a, ps.plan.blocks, ps.plan.smem,
+  SR_TRY_CUDA(ctx, sr::launch_interp(ps.plan.dpt, pred, ps.plan.ops, a, ps.plan.blocks, ps.plan.smem,
                                      ctx->stream));
   return SR_OK;
 }
@@ -288,8 +296,11 @@ std::string tune_key(const sr_context *ctx, const ProgramSet &ps) {
   const int lg_e = ps.E > 0 ? static_cast<int>(std::log2(static_cast<double>(ps.E))) : 0;
   const double mean_instr = ps.E > 0 ? static_cast<double>(ps.n_instr) / ps.E : 0.0;
   std::ostringstream k;
+  const bool prot = ps.n_instr > 0 &&
+                    static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr;
   k << ctx->device_name << "|V" << ctx->V << "|N" << lg_n << "|E" << lg_e << "|I"
-    << static_cast<int>(std::lround(std::log2(1.0 + mean_instr) * 4.0)) << "|S" << ps.smax;
+    << static_cast<int>(std::lround(std::log2(1.0 + mean_instr) * 4.0)) << "|S" << ps.smax
+    << "|P" << (prot ? sr::kOpsProtected : sr::kOpsAll);
   return k.str();
 }
 
@@ -1648,8 +1659,8 @@ sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
   SR_TRY_CUDA(ctx, ps.code.ensure(n_code));
   SR_TRY_CUDA(ctx, ps.off.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ps.len.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->evo_summary.ensure(6));
-  SR_TRY_CUDA(ctx, ctx->h_evo_summary.ensure(6));
+  SR_TRY_CUDA(ctx, ctx->evo_summary.ensure(8));
+  SR_TRY_CUDA(ctx, ctx->h_evo_summary.ensure(8));
   SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
   // The interpreter prefetches one instruction past a program: keep the
@@ -1658,7 +1669,7 @@ sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
   SR_TRY_CUDA(ctx, sr::launch_compile_device(tokens, values, lengths, E, stride, ctx->V,
                                              ps.code.p, ps.off.p, ps.len.p, ctx->evo_summary.p,
                                              ctx->stream));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_evo_summary.p, ctx->evo_summary.p, 6 * sizeof(int32_t),
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_evo_summary.p, ctx->evo_summary.p, 8 * sizeof(int32_t),
                                    cudaMemcpyDeviceToHost, ctx->stream));
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const int32_t *sm = ctx->h_evo_summary.p;
@@ -1672,6 +1683,7 @@ sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
   ps.smax = sm[0];
   ps.n_tokens = n_tok;
   ps.n_instr = n_ins;
+  ps.n_instr_protected = sm[6];
   ps.cost.assign(static_cast<size_t>(E), 0.0f);  // groups in population order
   ps.n_const.assign(static_cast<size_t>(E), 0);
   ps.sfu_per_dp = 0.0;

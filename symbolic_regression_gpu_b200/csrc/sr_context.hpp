@@ -77,6 +77,7 @@ struct PinnedBuf {
 struct Plan {
   int dpt = 8;
   int W = 8;           // evaluating warps per block
+  int ops = 0;         // operator profile dispatched inline (kOpsAll / kOpsProtected)
   int smax = 0;        // spill slots per warp
   int s_smem = 0;      // of which in shared memory
   int G = 0;           // expressions per group
@@ -105,6 +106,7 @@ struct ProgramSet {
   int E = 0;
   int smax = 0;
   int64_t n_instr = 0;
+  int64_t n_instr_protected = 0;  // instructions whose opcode kOpsProtected dispatches inline
   int64_t n_tokens = 0;      // tokens represented (skeleton-equivalent)
   double sfu_per_dp = 0.0;   // declared work, summed over expressions
   double fp32_per_dp = 0.0;
@@ -231,7 +233,7 @@ struct sr_context {
   sr::DevBuf<int32_t> evo_idx;     // [E]
   sr::DevBuf<int32_t> evo_order;   // [E]
   sr::DevBuf<float> evo_fit;       // [E] fitness in rank order
-  sr::DevBuf<int32_t> evo_summary; // [6] see launch_compile_device
+  sr::DevBuf<int32_t> evo_summary; // [8] see launch_compile_device
   sr::PinnedBuf<int32_t> h_evo_summary;
 
   // timing

@@ -24,7 +24,7 @@
 // two give the same distributions, not the same samples.  The order of draws
 // inside a child follows the reference's call order exactly (tournament,
 // mutation-or-crossover choice, node choice, generator), which the oracle
-// (oracle/oracle.py evolve_step) replays draw for draw.
+// (oracle/evolve.py) replays draw for draw.
 #include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -551,6 +551,9 @@ __global__ void compile_kernel(const int32_t *__restrict__ tok, const float *__r
     return;
   }
   code_len[i] = count;
+  int prot = 0;
+  for (int k = 0; k < count; ++k) prot += in_protected_profile(instr_op(code[base + k].w)) ? 1 : 0;
+  if (prot) atomicAdd(&summary[6], prot);
   atomicMax(&summary[0], need);
   atomicAdd(reinterpret_cast<unsigned long long *>(summary + 2), static_cast<unsigned long long>(n));
   atomicAdd(reinterpret_cast<unsigned long long *>(summary + 4),
@@ -608,7 +611,7 @@ cudaError_t launch_compile_device(const int32_t *tok, const float *val, const in
                                   int E, int stride, int num_vars, Instr *code,
                                   int64_t *code_off, int32_t *code_len, int32_t *summary,
                                   cudaStream_t s) {
-  cudaError_t err = cudaMemsetAsync(summary, 0, 6 * sizeof(int32_t), s);
+  cudaError_t err = cudaMemsetAsync(summary, 0, 8 * sizeof(int32_t), s);
   if (err != cudaSuccess || E <= 0) return err;
   compile_kernel<<<grid_for(E, 64), 64, 0, s>>>(tok, val, len, E, stride, num_vars, code,
                                                 code_off, code_len, summary);

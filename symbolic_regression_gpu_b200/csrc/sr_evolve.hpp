@@ -55,8 +55,8 @@ cudaError_t launch_evolve_step(const EvolveParams &p, int generation, int E, int
 // bytecode: program i at code[i * (stride + 1)], code_off / code_len per
 // expression.  summary[0] = largest spill-slot need, summary[1] = error flag
 // (1 = an invalid expression; its code_len is 0), summary[2..3] = total
-// tokens (int64), summary[4..5] = total instructions (int64); zeroed by the
-// launcher.
+// tokens (int64), summary[4..5] = total instructions (int64), summary[6] =
+// instructions inside the kOpsProtected profile; zeroed by the launcher.
 cudaError_t launch_compile_device(const int32_t *tok, const float *val, const int32_t *len,
                                   int E, int stride, int num_vars, Instr *code,
                                   int64_t *code_off, int32_t *code_len, int32_t *summary,

@@ -81,6 +81,22 @@ SR_HD bool is_unary_token(int tok) {
   return (tok >= 10 && tok <= 27) || tok == static_cast<int>(kOpExpClamp);
 }
 
+// Operator profiles of the interpreter: the set of opcodes its dispatch
+// switch handles inline (every other opcode goes through one out-of-line
+// routine, with identical results).  kOpsProtected: + - *, protected
+// division, sin, cos, exp clamped at 80, protected log and sqrt|x| (and their
+// reversed forms); kOpsAll: the arithmetic, divisions, roots, reciprocal,
+// sin / cos / exp / log families.  A launch uses kOpsProtected when at least
+// kProtectedShare of its instructions are in it.
+constexpr int kOpsAll = 0;
+constexpr int kOpsProtected = 1;
+constexpr double kProtectedShare = 0.9;
+SR_HD bool in_protected_profile(uint32_t op) {
+  return op == 0 || op == 1 || op == 2 || op == kOpReversed + 2 || op == 3 || op == 8 ||
+         op == kOpReversed + 8 || op == 10 || op == 11 || op == kOpExpClamp || op == 22 ||
+         op == 27;
+}
+
 // Device-side error word bits.
 enum : int32_t {
   kDevErrTimeout = 1,   // a bounded mbarrier wait gave up

@@ -1,6 +1,9 @@
 // sr_kernels.cu — sm_100a kernels of the population evaluator.
 //
-//  interp_kernel<DPT, PRED>   persistent interpreter.  One producer thread
+//  interp_kernel<DPT, PRED, MAXW, MINB, OPS>
+//                             persistent interpreter (OPS: the operator
+//                             profile its switch dispatches inline,
+//                             sr_internal.hpp).  One producer thread
 //                             per block claims work items (span, group) from
 //                             a global counter and copies the item's X span
 //                             (every row) into one of two shared-memory
@@ -40,7 +43,7 @@ namespace {
 
 // MAXW / MINB: launch bounds of the instantiation (at most MAXW evaluating
 // warps, at least MINB resident blocks per SM), which set the register budget.
-template <int DPT, bool PRED, int MAXW, int MINB>
+template <int DPT, bool PRED, int MAXW, int MINB, int OPS>
 __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const EvalArgs p) {
   constexpr int TILE = 32 * DPT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -104,7 +107,7 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
         if (dp0 >= p.N) break;  // tail of the last span
         const float *xs = xb + t * TILE;
         float T[DPT];
-        run_program<DPT>(code, len, xs, span, st, lane, p.cache, p.ldc, dp0, T);
+        run_program<DPT, OPS>(code, len, xs, span, st, lane, p.cache, p.ldc, dp0, T);
         if constexpr (PRED) {
           stg_vec<DPT>(p.pred + static_cast<int64_t>(p.pred_row[e]) * p.ldp + dp0, lane, T);
         } else {
@@ -295,33 +298,40 @@ size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span) {
          kBufs * sizeof(ItemDesc) + 2 * kBufs * sizeof(uint64_t);
 }
 
-template <int DPT, bool PRED, int MAXW, int MINB>
+template <int DPT, bool PRED, int MAXW, int MINB, int OPS = kOpsAll>
 static const void *interp_fn() {
-  return reinterpret_cast<const void *>(&interp_kernel<DPT, PRED, MAXW, MINB>);
+  return reinterpret_cast<const void *>(&interp_kernel<DPT, PRED, MAXW, MINB, OPS>);
+}
+
+template <int DPT, int MAXW, int MINB>
+static const void *interp_mse(int ops) {
+  return ops == kOpsProtected ? interp_fn<DPT, false, MAXW, MINB, kOpsProtected>()
+                              : interp_fn<DPT, false, MAXW, MINB, kOpsAll>();
 }
 
 // Instantiations: W <= 8 uses the narrow variants (more blocks per SM, tighter
-// register budget), larger W the wide ones.
-static const void *select_interp(int dpt, bool pred, int W) {
+// register budget), larger W the wide ones.  MSE launches come in both
+// operator profiles, prediction launches in kOpsAll.
+static const void *select_interp(int dpt, bool pred, int ops, int W) {
   const bool narrow = W <= 8;
   if (dpt == 16) {
-    if (narrow) return pred ? interp_fn<16, true, 8, 2>() : interp_fn<16, false, 8, 2>();
-    return pred ? interp_fn<16, true, 16, 1>() : interp_fn<16, false, 16, 1>();
+    if (narrow) return pred ? interp_fn<16, true, 8, 2>() : interp_mse<16, 8, 2>(ops);
+    return pred ? interp_fn<16, true, 16, 1>() : interp_mse<16, 16, 1>(ops);
   }
   if (dpt == 8) {
-    if (narrow) return pred ? interp_fn<8, true, 8, 3>() : interp_fn<8, false, 8, 3>();
-    return pred ? interp_fn<8, true, 16, 1>() : interp_fn<8, false, 16, 1>();
+    if (narrow) return pred ? interp_fn<8, true, 8, 3>() : interp_mse<8, 8, 3>(ops);
+    return pred ? interp_fn<8, true, 16, 1>() : interp_mse<8, 16, 1>(ops);
   }
   if (dpt == 4) {
-    if (narrow) return pred ? interp_fn<4, true, 8, 4>() : interp_fn<4, false, 8, 4>();
-    return pred ? interp_fn<4, true, 16, 2>() : interp_fn<4, false, 16, 2>();
+    if (narrow) return pred ? interp_fn<4, true, 8, 4>() : interp_mse<4, 8, 4>(ops);
+    return pred ? interp_fn<4, true, 16, 2>() : interp_mse<4, 16, 2>(ops);
   }
   return nullptr;
 }
 
-cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
+cudaError_t interp_configure(int dpt, bool pred, int ops, size_t smem, int W,
                              int *blocks_per_sm) {
-  const void *fn = select_interp(dpt, pred, W);
+  const void *fn = select_interp(dpt, pred, ops, W);
   if (!fn || W < 1 || W > kMaxWarps) return cudaErrorInvalidValue;
   cudaError_t err = cudaFuncSetAttribute(
       fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -330,9 +340,9 @@ cudaError_t interp_configure(int dpt, bool pred, size_t smem, int W,
                                                        (W + 1) * 32, smem);
 }
 
-cudaError_t launch_interp(int dpt, bool pred, const EvalArgs &args, int blocks,
+cudaError_t launch_interp(int dpt, bool pred, int ops, const EvalArgs &args, int blocks,
                           size_t smem, cudaStream_t stream) {
-  const void *fn = select_interp(dpt, pred, args.W);
+  const void *fn = select_interp(dpt, pred, ops, args.W);
   if (!fn || args.W < 1 || args.W > kMaxWarps) return cudaErrorInvalidValue;
   // Plans of one instantiation can differ in shared-memory size (main and
   // cache-fill sets, autotune candidates); the attribute belongs to the

@@ -324,3 +324,27 @@ def test_ieee_only_long_trees_bit_exact(evaluator):
     ref = oracle.predict_f32(pop, X)
     bad = [i for i in range(pop.num_exprs) if not same_float(pred[i], ref[i]).all()]
     assert not bad, bad
+
+
+def test_operator_profiles_give_identical_results():
+    """A launch dominated by the protected operator set runs the kOpsProtected
+    interpreter (other operators out of line), a mixed one kOpsAll: the same
+    expression gets the same MSE bits either way."""
+    rng = np.random.default_rng(77)
+    V, N = 3, 20_000
+    X = np.empty((V + 1, N), np.float32)
+    X[:V] = rng.uniform(-3, 3, size=(V, N))
+    X[V] = np.sin(X[0]) * X[1] + 0.1
+    prot = synth.TreeGen(rng, V, p_const=0.3, binary=(1, 2, 3, 8), unary=(10, 11, 32, 22, 27))
+    rare = synth.TreeGen(rng, V, p_const=0.3, binary=(4, 5, 6, 7, 9), unary=tuple(range(12, 22)))
+    mixed = synth.TreeGen(rng, V, p_const=0.3, binary=tuple(range(1, 10)),
+                          unary=tuple(range(10, 28)) + (32,))
+    base = [prot.depth_tree(6, full=False) for _ in range(400)]
+    base += [mixed.depth_tree(4, full=False) for _ in range(8)]   # a few rare operators
+    extra = [rare.depth_tree(6, full=False) for _ in range(600)]
+    with sg.Evaluator(device=0) as ev:
+        ev.set_data(X)
+        a = ev.eval_mse(Population.from_lists(base))
+        b = ev.eval_mse(Population.from_lists(base + extra))[:len(base)]
+    same = (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
+    assert same.all()
