@@ -1280,6 +1280,18 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     cl.seg_cap = std::min(sr::adj_segment(), maxlen);
     cl.tape_len = tape_len;
     cl.gmax = std::max(cg, 1);
+    {
+      int64_t n_in = 0, n_prot = 0;
+      for (int32_t x : mem) {
+        const Instr *code = ps.h_code.p + ps.h_off.p[x];
+        for (int i = 0; i < ps.h_len.p[x]; ++i)
+          n_prot += sr::in_protected_profile(sr::instr_op(code[i].w)) ? 1 : 0;
+        n_in += ps.h_len.p[x];
+      }
+      cl.plan.ops = (n_in > 0 && static_cast<double>(n_prot) >= sr::kProtectedShare * n_in)
+                        ? sr::kOpsProtected
+                        : sr::kOpsAll;
+    }
     // Most resident evaluating warps per SM.  A shared-memory tape costs
     // occupancy (every warp holds its whole tape), a global one costs L2
     // traffic (each tape entry is written and read back once per tile, by the
@@ -1291,12 +1303,12 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     size_t best_smem = 0;
     for (int pass = 0; pass < 2; ++pass) {
       const bool gt = (pass == 1);
-      for (int W = sr::kMaxWarps; W >= 1; --W) {
+      for (int W = sr::adj_max_warps(recompute); W >= 1; --W) {
         const size_t smem =
             sr::adj_smem_bytes(W, ctx->V, s_smem, g.span, cl.tape_len, cl.gmax, gt);
         if (smem > static_cast<size_t>(dev_max_smem)) continue;
         int bps = 0;
-        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, &bps));
+        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, cl.plan.ops, &bps));
         if (bps <= 0) continue;
         const int64_t resident_tape =
             static_cast<int64_t>(W) * bps * ctx->num_sms * cl.tape_len * tile * 4;
@@ -1406,7 +1418,7 @@ sr_status launch_grad(sr_context *ctx) {
     a.seg_cap = cl.seg_cap;
     a.gmax = cl.gmax;
     SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.blocks, cl.plan.smem, s));
+    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.ops, cl.plan.blocks, cl.plan.smem, s));
   }
   SR_TRY_CUDA(ctx, record_event(ctx, 2));
   SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E, g.const_off.p,
