@@ -2,8 +2,7 @@
 // every expression's constants, and on-device Adam over those constants.
 // (No reference counterpart: the reference evaluates MSE only.)
 //
-//   adj_kernel<GTAPE, RECOMP, OPS>
-//                           fused forward + backward per tile.  Same work
+//   adj_kernel<GTAPE>       fused forward + backward per tile.  Same work
 //                           decomposition as interp_kernel (a producer thread
 //                           streaming X spans into shared memory, warps
 //                           claiming expressions of a group).  Per tile a warp
@@ -305,7 +304,7 @@ __device__ __forceinline__ void binary_vd(int which, const float (&u)[DPT], cons
   break;
 
 template <int DPT>
-__device__ __forceinline__ void apply_op_grad_any(uint32_t op, float (&T)[DPT], float (&b)[DPT],
+__device__ __forceinline__ void apply_op_grad(uint32_t op, float (&T)[DPT], float (&b)[DPT],
                                               float (&dT)[DPT], float (&db)[DPT]) {
   bool flat[DPT];
 #pragma unroll
@@ -372,84 +371,6 @@ __device__ __forceinline__ void apply_op_grad_any(uint32_t op, float (&T)[DPT], 
     default: SR_EACH2(T[k] = 0.0f; dT[k] = 0.0f; db[k] = 0.0f)
   }
 }
-
-// Out-of-line entry of the operators outside a launch's profile (values and
-// partials through the caller's stack, copies).
-template <int DPT>
-__device__ __noinline__ void apply_op_grad_cold(uint32_t op, float *T, float *b, float *dT,
-                                                float *db) {
-  float t[DPT], bb[DPT], dt[DPT], dbb[DPT];
-#pragma unroll
-  for (int k = 0; k < DPT; ++k) {
-    t[k] = T[k];
-    bb[k] = b[k];
-  }
-  apply_op_grad_any<DPT>(op, t, bb, dt, dbb);
-#pragma unroll
-  for (int k = 0; k < DPT; ++k) {
-    T[k] = t[k];
-    dT[k] = dt[k];
-    db[k] = dbb[k];
-  }
-}
-
-// T = op(T, b) with its partials.  kOpsAll dispatches every operator inline;
-// kOpsProtected only the protected set (sr_internal.hpp), the rest out of
-// line (a compact hot switch: the interpreter's instruction-cache lesson).
-template <int DPT, int OPS>
-__device__ __forceinline__ void apply_op_grad(uint32_t op, float (&T)[DPT], float (&b)[DPT],
-                                              float (&dT)[DPT], float (&db)[DPT]) {
-  if constexpr (OPS == kOpsProtected) {
-    bool flat[DPT];
-#pragma unroll
-    for (int k = 0; k < DPT; ++k) flat[k] = false;
-    switch (op) {
-    case 0: SR_EACH2(dT[k] = 1.0f)
-    case 1: SR_EACH2(T[k] = __fadd_rn(T[k], b[k]); dT[k] = 1.0f; db[k] = 1.0f)
-    case 2: SR_EACH2(T[k] = __fsub_rn(T[k], b[k]); dT[k] = 1.0f; db[k] = -1.0f)
-    case 42: SR_EACH2(T[k] = __fsub_rn(b[k], T[k]); dT[k] = -1.0f; db[k] = 1.0f)
-    case 3: SR_EACH2(db[k] = T[k]; dT[k] = b[k]; T[k] = __fmul_rn(T[k], b[k]))
-    case 8: {  // T / protected(b)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        flat[k] = fabsf(b[k]) <= 1e-9f;
-        b[k] = loose_denom(b[k]);
-      }
-    }
-      SR_G2(2, false, false)
-    case 48: {  // b / protected(T)
-#pragma unroll
-      for (int k = 0; k < DPT; ++k) {
-        flat[k] = fabsf(T[k]) <= 1e-9f;
-        T[k] = loose_denom(T[k]);
-      }
-    }
-      SR_G2(2, true, false)
-    case 10: SR_G1(g_sin)
-    case 11: SR_G1(g_cos)
-    case 22: SR_G1(g_llog)
-    case 27: SR_G1(g_lsqrt)
-    case 32: SR_G1(g_expc)
-      default: {
-        float t_[DPT], b_[DPT], dt_[DPT], db_[DPT];
-#pragma unroll
-        for (int k = 0; k < DPT; ++k) {
-          t_[k] = T[k];
-          b_[k] = b[k];
-        }
-        apply_op_grad_cold<DPT>(op, t_, b_, dt_, db_);
-#pragma unroll
-        for (int k = 0; k < DPT; ++k) {
-          T[k] = t_[k];
-          dT[k] = dt_[k];
-          db[k] = db_[k];
-        }
-      } break;
-    }
-  } else {
-    apply_op_grad_any<DPT>(op, T, b, dT, db);
-  }
-}
 #undef SR_G1
 #undef SR_G2
 #undef SR_EACH2
@@ -473,7 +394,7 @@ __device__ __forceinline__ bool needs_db(uint32_t bk) { return bk == kBC || bk =
 
 // One forward instruction: [spill] [T = leaf] [b = operand] T = op(T, b),
 // with its local partials in dT / db.  Returns the operand kind of b.
-template <int DPT, int OPS>
+template <int DPT>
 __device__ __forceinline__ uint32_t fwd_instr(const uint4 ins, float (&T)[DPT], float (&dT)[DPT],
                                               float (&db)[DPT], const float *xs, int span,
                                               const SpillStack &st, int lane, const EvalArgs &p,
@@ -485,7 +406,7 @@ __device__ __forceinline__ uint32_t fwd_instr(const uint4 ins, float (&T)[DPT], 
   float b[DPT];
   const uint32_t bk = instr_b_kind(w);
   if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, span, st, lane, p.cache, p.ldc, dp0);
-  apply_op_grad<DPT, OPS>(instr_op(w), T, b, dT, db);
+  apply_op_grad<DPT>(instr_op(w), T, b, dT, db);
   return bk;
 }
 
@@ -538,13 +459,8 @@ __device__ __forceinline__ void bwd_instr(const uint4 ins, float (&gT)[DPT], con
 // spill slots (smax), checkpoints ((segments - 1) x (1 + smax)).
 constexpr int kSeg = 16;
 
-// Launch bounds: checkpoint mode at most kAdjMaxWarpsCkpt evaluating warps
-// and two resident blocks per SM (registers capped near 80: 22 warps per SM;
-// the kernel is latency-bound, so warps matter more than registers);
-// recompute mode, whose replay needs more registers, up to kMaxWarps with one.
-template <bool GTAPE, bool RECOMP, int OPS>
-__global__ void __launch_bounds__((RECOMP ? kMaxWarps : kAdjMaxWarpsCkpt) * 32 + 32,
-                                  RECOMP ? 1 : 2) adj_kernel(const AdjArgs a) {
+template <bool GTAPE, bool RECOMP>
+__global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjArgs a) {
   constexpr int DPT = kAdjDpt;
   constexpr int TILE = 32 * DPT;
   const EvalArgs &p = a.e;
@@ -650,7 +566,7 @@ __global__ void __launch_bounds__((RECOMP ? kMaxWarps : kAdjMaxWarpsCkpt) * 32 +
               }
             }
             float dT[DPT], db[DPT];
-            const uint32_t bk = fwd_instr<DPT, OPS>(ins, T, dT, db, xs, span, st, lane, p, dp0);
+            const uint32_t bk = fwd_instr<DPT>(ins, T, dT, db, xs, span, st, lane, p, dp0);
             if (i >= t_lo) {
               sts_vec<DPT>(tape + (i - (RECOMP ? last_seg : lo)) * TILE, lane, dT);
               if (needs_db(bk)) {
@@ -723,7 +639,7 @@ __global__ void __launch_bounds__((RECOMP ? kMaxWarps : kAdjMaxWarpsCkpt) * 32 +
               for (int i = s0; i < s1; ++i) {
                 const uint4 ins = ldg_instr(code + i);
                 float dT[DPT], db[DPT];
-                const uint32_t bk = fwd_instr<DPT, OPS>(ins, T, dT, db, xs, span, st, lane, p, dp0);
+                const uint32_t bk = fwd_instr<DPT>(ins, T, dT, db, xs, span, st, lane, p, dp0);
                 if (i >= lo) {
                   sts_vec<DPT>(tape + (i - s0) * TILE, lane, dT);
                   if (needs_db(bk)) {
@@ -825,33 +741,27 @@ size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax
          2 * kBufs * sizeof(uint64_t);
 }
 
-template <int OPS>
-static const void *adj_fn_ops(bool global_tape, bool recompute) {
+static const void *adj_fn(bool global_tape, bool recompute) {
   if (recompute)
-    return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true, true, OPS>)
-                       : reinterpret_cast<const void *>(&adj_kernel<false, true, OPS>);
-  return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true, false, OPS>)
-                     : reinterpret_cast<const void *>(&adj_kernel<false, false, OPS>);
+    return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true, true>)
+                       : reinterpret_cast<const void *>(&adj_kernel<false, true>);
+  return global_tape ? reinterpret_cast<const void *>(&adj_kernel<true, false>)
+                     : reinterpret_cast<const void *>(&adj_kernel<false, false>);
 }
 
-static const void *adj_fn(bool global_tape, bool recompute, int ops) {
-  return ops == kOpsProtected ? adj_fn_ops<kOpsProtected>(global_tape, recompute)
-                              : adj_fn_ops<kOpsAll>(global_tape, recompute);
-}
-
-cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute, int ops,
+cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute,
                           int *blocks_per_sm) {
-  const void *fn = adj_fn(global_tape, recompute, ops);
+  const void *fn = adj_fn(global_tape, recompute);
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, (W + 1) * 32, smem);
 }
 
-cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int ops, int blocks, size_t smem,
+cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int blocks, size_t smem,
                            cudaStream_t stream) {
-  if (args.e.W < 1 || args.e.W > adj_max_warps(recompute)) return cudaErrorInvalidValue;
-  const void *fn = adj_fn(args.gtape != nullptr, recompute, ops);
+  if (args.e.W < 1 || args.e.W > kMaxWarps) return cudaErrorInvalidValue;
+  const void *fn = adj_fn(args.gtape != nullptr, recompute);
   // Each tape class has its own shared-memory size; the attribute is the
   // kernel's, so set it for this launch.
   const cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,

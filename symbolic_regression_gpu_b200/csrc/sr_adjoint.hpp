@@ -23,20 +23,15 @@ struct AdjArgs {
   int32_t reserved0;
 };
 
-// Evaluating warps per block of the adjoint kernel (its launch bounds):
-// checkpoint mode kAdjMaxWarpsCkpt, recompute mode kMaxWarps.
-constexpr int kAdjMaxWarpsCkpt = 11;
-inline int adj_max_warps(bool recompute) { return recompute ? kMaxWarps : kAdjMaxWarpsCkpt; }
 // Datapoints per thread of the adjoint kernel.
 int adj_dpt();
 size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax,
                       bool global_tape);
 // Instructions per recompute segment.
 int adj_segment();
-// `ops`: operator profile dispatched inline (kOpsAll / kOpsProtected).
-cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute, int ops,
+cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute,
                           int *blocks_per_sm);
-cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int ops, int blocks, size_t smem,
+cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int blocks, size_t smem,
                            cudaStream_t stream);
 cudaError_t launch_grad_finalize(const double2 *partial, int n_spans, int E,
                                  const int64_t *const_off, const int32_t *const_cnt,

@@ -145,9 +145,15 @@ sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *
   }
   ps.h_code.p[total] = Instr{0, 0, 0, 0};  // prefetch padding
   int64_t in_profile = 0;
-  for (int64_t i = 0; i < total; ++i)
-    in_profile += sr::in_protected_profile(sr::instr_op(ps.h_code.p[i].w)) ? 1 : 0;
+  bool cache_refs = false;
+  for (int64_t i = 0; i < total; ++i) {
+    const uint32_t w = ps.h_code.p[i].w;
+    in_profile += sr::in_protected_profile(sr::instr_op(w)) ? 1 : 0;
+    cache_refs = cache_refs || (sr::instr_load(w) && sr::instr_leaf_kind(w) == sr::kLeafR) ||
+                 sr::instr_b_kind(w) == sr::kBR;
+  }
   ps.n_instr_protected = in_profile;
+  ps.cache_refs = cache_refs;
   int64_t o = 0;
   for (int x = 0; x < E; ++x) {
     const auto &in = infos[static_cast<size_t>(x)];
@@ -175,6 +181,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
            static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr)
               ? sr::kOpsProtected
               : sr::kOpsAll;
+  p.cache = !pred && ps.cache_refs;
   p.smax = std::max(ps.smax, 0);
   p.s_smem = std::min(p.smax, sr::smem_spill_slots(dpt));
   const int64_t tile = 32 * dpt;
@@ -200,7 +207,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   if (!pred && static_cast<double>(p.n_spans) * E * 16.0 > 8.0 * (1ull << 30))
     return ctx->fail(SR_ERR_UNSUPPORTED, "partial-sum buffer would exceed 8 GiB");
   int bps = 0;
-  SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.smem, W, &bps));
+  SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache, p.smem, W, &bps));
   if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
   const int64_t resident = static_cast<int64_t>(bps) * ctx->num_sms;
   p.blocks = static_cast<int>(std::min<int64_t>(resident, std::max<int64_t>(p.items(), 1)));
@@ -284,7 +291,8 @@ sr_status launch_set(sr_context *ctx, ProgramSet &ps, bool pred, int32_t *counte
   a.ldp = ldp;
   a.pred_row = pred_row;
   SR_TRY_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int32_t), ctx->stream));
-  SR_TRY_CUDA(ctx, sr::launch_interp(ps.plan.dpt, pred, ps.plan.ops, a, ps.plan.blocks, ps.plan.smem,
+  SR_TRY_CUDA(ctx, sr::launch_interp(ps.plan.dpt, pred, ps.plan.ops, ps.plan.cache, a,
+                                     ps.plan.blocks, ps.plan.smem,
                                      ctx->stream));
   return SR_OK;
 }
@@ -1280,18 +1288,6 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     cl.seg_cap = std::min(sr::adj_segment(), maxlen);
     cl.tape_len = tape_len;
     cl.gmax = std::max(cg, 1);
-    {
-      int64_t n_in = 0, n_prot = 0;
-      for (int32_t x : mem) {
-        const Instr *code = ps.h_code.p + ps.h_off.p[x];
-        for (int i = 0; i < ps.h_len.p[x]; ++i)
-          n_prot += sr::in_protected_profile(sr::instr_op(code[i].w)) ? 1 : 0;
-        n_in += ps.h_len.p[x];
-      }
-      cl.plan.ops = (n_in > 0 && static_cast<double>(n_prot) >= sr::kProtectedShare * n_in)
-                        ? sr::kOpsProtected
-                        : sr::kOpsAll;
-    }
     // Most resident evaluating warps per SM.  A shared-memory tape costs
     // occupancy (every warp holds its whole tape), a global one costs L2
     // traffic (each tape entry is written and read back once per tile, by the
@@ -1303,12 +1299,12 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     size_t best_smem = 0;
     for (int pass = 0; pass < 2; ++pass) {
       const bool gt = (pass == 1);
-      for (int W = sr::adj_max_warps(recompute); W >= 1; --W) {
+      for (int W = sr::kMaxWarps; W >= 1; --W) {
         const size_t smem =
             sr::adj_smem_bytes(W, ctx->V, s_smem, g.span, cl.tape_len, cl.gmax, gt);
         if (smem > static_cast<size_t>(dev_max_smem)) continue;
         int bps = 0;
-        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, cl.plan.ops, &bps));
+        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, &bps));
         if (bps <= 0) continue;
         const int64_t resident_tape =
             static_cast<int64_t>(W) * bps * ctx->num_sms * cl.tape_len * tile * 4;
@@ -1418,7 +1414,7 @@ sr_status launch_grad(sr_context *ctx) {
     a.seg_cap = cl.seg_cap;
     a.gmax = cl.gmax;
     SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.ops, cl.plan.blocks, cl.plan.smem, s));
+    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.blocks, cl.plan.smem, s));
   }
   SR_TRY_CUDA(ctx, record_event(ctx, 2));
   SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E, g.const_off.p,
@@ -1696,6 +1692,7 @@ sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
   ps.n_tokens = n_tok;
   ps.n_instr = n_ins;
   ps.n_instr_protected = sm[6];
+  ps.cache_refs = false;  // compiled without cache hints
   ps.cost.assign(static_cast<size_t>(E), 0.0f);  // groups in population order
   ps.n_const.assign(static_cast<size_t>(E), 0);
   ps.sfu_per_dp = 0.0;

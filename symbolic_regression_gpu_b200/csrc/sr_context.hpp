@@ -78,6 +78,7 @@ struct Plan {
   int dpt = 8;
   int W = 8;           // evaluating warps per block
   int ops = 0;         // operator profile dispatched inline (kOpsAll / kOpsProtected)
+  bool cache = false;  // programs read cached subtrees (cached-operand paths compiled in)
   int smax = 0;        // spill slots per warp
   int s_smem = 0;      // of which in shared memory
   int G = 0;           // expressions per group
@@ -107,6 +108,7 @@ struct ProgramSet {
   int smax = 0;
   int64_t n_instr = 0;
   int64_t n_instr_protected = 0;  // instructions whose opcode kOpsProtected dispatches inline
+  bool cache_refs = false;        // some instruction reads a cached subtree
   int64_t n_tokens = 0;      // tokens represented (skeleton-equivalent)
   double sfu_per_dp = 0.0;   // declared work, summed over expressions
   double fp32_per_dp = 0.0;

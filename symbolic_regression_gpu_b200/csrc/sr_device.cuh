@@ -268,14 +268,16 @@ __device__ __forceinline__ void unquad(float (&v)[DPT], int h, float4 q) {
   v[4 * h + 3] = q.w;
 }
 
-// T = leaf; kind and payload are warp-uniform.
-template <int DPT>
+// T = leaf; kind and payload are warp-uniform.  CACHE = false compiles out
+// the cached-subtree kind (programs compiled without cache hints have none),
+// which keeps the dispatch code compact.
+template <int DPT, bool CACHE = true>
 __device__ __forceinline__ void load_leaf(uint32_t kind, uint32_t payload, float (&T)[DPT],
                                           const float *xs, int xrs, int lane,
                                           const float *cache, int64_t ldc, int64_t dp0) {
   if (kind == kLeafX) {
     lds_vec<DPT>(xs + payload * xrs, lane, T);
-  } else if (kind == kLeafC) {
+  } else if (!CACHE || kind == kLeafC) {
     const float c = __uint_as_float(payload);
 #pragma unroll
     for (int k = 0; k < DPT; ++k) T[k] = c;
@@ -293,14 +295,42 @@ struct SpillStack {
   int s_smem;
 };
 
+// Slots in global scratch are rare (deep expressions only): their copies
+// run out of line, through stack copies of the lane's values, to keep the
+// dispatch code compact.
+template <int DPT>
+__device__ __noinline__ void spill_store_global(float *dst, int lane, const float *src) {
+  float v[DPT];
+#pragma unroll
+  for (int k = 0; k < DPT; ++k) v[k] = src[k];
+  stg_vec<DPT>(dst, lane, v);
+}
+
+template <int DPT>
+__device__ __noinline__ void spill_load_global(const float *src, int lane, float *dst) {
+  // Plain (coherent) loads: the data was written by this warp in this kernel.
+#pragma unroll
+  for (int h = 0; h < DPT / 4; ++h) {
+    const float4 q = *reinterpret_cast<const float4 *>(src + h * 128 + lane * 4);
+    dst[4 * h + 0] = q.x;
+    dst[4 * h + 1] = q.y;
+    dst[4 * h + 2] = q.z;
+    dst[4 * h + 3] = q.w;
+  }
+}
+
 template <int DPT>
 __device__ __forceinline__ void spill_store(const SpillStack &st, uint32_t slot, int lane,
                                             const float (&T)[DPT]) {
   constexpr int TILE = 32 * DPT;
-  if (static_cast<int>(slot) < st.s_smem)
+  if (static_cast<int>(slot) < st.s_smem) {
     sts_vec<DPT>(st.ss + slot * TILE, lane, T);
-  else
-    stg_vec<DPT>(st.gs + (slot - st.s_smem) * TILE, lane, T);
+  } else {
+    float t[DPT];
+#pragma unroll
+    for (int k = 0; k < DPT; ++k) t[k] = T[k];
+    spill_store_global<DPT>(st.gs + (slot - st.s_smem) * TILE, lane, t);
+  }
 }
 
 template <int DPT>
@@ -310,21 +340,15 @@ __device__ __forceinline__ void spill_load(const SpillStack &st, uint32_t slot, 
   if (static_cast<int>(slot) < st.s_smem) {
     lds_vec<DPT>(st.ss + slot * TILE, lane, v);
   } else {
-    // Plain (coherent) loads: the data was written by this warp in this kernel.
-    const float *base = st.gs + (slot - st.s_smem) * TILE;
+    float t[DPT];
+    spill_load_global<DPT>(st.gs + (slot - st.s_smem) * TILE, lane, t);
 #pragma unroll
-    for (int h = 0; h < DPT / 4; ++h) {
-      const float4 q = *reinterpret_cast<const float4 *>(base + h * 128 + lane * 4);
-      v[4 * h + 0] = q.x;
-      v[4 * h + 1] = q.y;
-      v[4 * h + 2] = q.z;
-      v[4 * h + 3] = q.w;
-    }
+    for (int k = 0; k < DPT; ++k) v[k] = t[k];
   }
 }
 
 // b = operand; kind and payload are warp-uniform, kind != kBNone.
-template <int DPT>
+template <int DPT, bool CACHE = true>
 __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, float (&b)[DPT],
                                              const float *xs, int xrs, const SpillStack &st,
                                              int lane, const float *cache, int64_t ldc,
@@ -333,7 +357,7 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
     const float c = __uint_as_float(payload);
 #pragma unroll
     for (int k = 0; k < DPT; ++k) b[k] = c;
-  } else if (kind == kBR) {
+  } else if (CACHE && kind == kBR) {
     ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, b);
   } else if (kind == kBX) {
     lds_vec<DPT>(xs + payload * xrs, lane, b);
@@ -450,21 +474,17 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
   }                                                                            \
     SR_CALL1(v_exp)
 
-// Operator profiles.  The interpreter dispatches the operators of its
-// profile inline and every other one through apply_op_cold, one out-of-line
-// routine with the complete switch.  Keeping cases out of the inline switch
-// keeps the interpreter's hot code compact (instruction-cache pressure): on
-// the batched population (whose operators are those of kOpsProtected) the
-// forward launch took 95.6 ms with every case inline, 89.6 ms with kOpsAll's
-// inline set and 82.9 ms with kOpsProtected's.
-//   kOpsAll        arithmetic, MIN / MAX, ABS / NEG, divisions, roots, the
-//                  reciprocal, sin / cos / exp / log and their protected forms
-//                  (powers, tan, hyperbolic and inverse trigonometric
-//                  functions out of line);
-//   kOpsProtected  + - *, protected division, sin, cos, exp clamped at 80,
-//                  protected log and sqrt|x| (the evolution workloads' set).
-// (kOpsAll / kOpsProtected and the host-side membership test live in
-// sr_internal.hpp.)
+// Operator profiles (kOpsAll / kOpsProtected and the host-side membership
+// test live in sr_internal.hpp).  kOpsAll dispatches every operator inline;
+// kOpsProtected dispatches + - *, protected division, sin, cos, exp clamped
+// at 80, protected log and sqrt|x| (the evolution workloads' set) inline and
+// every other operator through apply_op_cold, one out-of-line routine with
+// the complete switch.  Keeping cases out of the inline switch keeps the
+// interpreter's hot code compact (instruction-cache pressure): on the batched
+// population, whose operators are kOpsProtected's, the forward launch took
+// 95.6 ms with every case inline and 82.9 ms with kOpsProtected's inline set;
+// a population that uses every operator (the reference generator's) runs
+// faster with all of them inline.
 
 template <int DPT>
 __device__ __forceinline__ void apply_op_any(uint32_t op, float (&T)[DPT], float (&b)[DPT]) {
@@ -514,12 +534,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
       SR_C_COLD
     }
   } else {
-    switch (op) {
-      SR_C_NONE SR_C_ADD SR_C_SUB SR_C_RSUB SR_C_MUL SR_C_DIV SR_C_RDIV SR_C_MIN SR_C_RMIN
-      SR_C_MAX SR_C_RMAX SR_C_LDIV SR_C_RLDIV SR_C_SIN SR_C_COS SR_C_EXP SR_C_LOG SR_C_INV
-      SR_C_LLOG SR_C_LINV SR_C_ABS SR_C_NEG SR_C_SQRT SR_C_LSQRT SR_C_EXPC
-      SR_C_COLD
-    }
+    apply_op_any<DPT>(op, T, b);
   }
 }
 
@@ -531,7 +546,7 @@ __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b
 // Run one compiled program over the warp's DPT x 32 datapoints of a tile.
 // xs points at the tile's first datapoint of X row 0; rows are xrs floats
 // apart.
-template <int DPT, int OPS>
+template <int DPT, int OPS, bool CACHE>
 __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
                                             int len, const float *xs, int xrs,
                                             const SpillStack &st, int lane,
@@ -546,13 +561,30 @@ __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
     const uint32_t w = ins.x;
     if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
     if (instr_load(w))
-      load_leaf<DPT>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
+      load_leaf<DPT, CACHE>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
     float b[DPT];
     const uint32_t bk = instr_b_kind(w);
-    if (bk != kBNone) load_operand<DPT>(bk, ins.z, b, xs, xrs, st, lane, cache, ldc, dp0);
+    if (bk != kBNone) load_operand<DPT, CACHE>(bk, ins.z, b, xs, xrs, st, lane, cache, ldc, dp0);
     apply_op<DPT, OPS>(instr_op(w), T, b);
     ins = nxt;
   }
+}
+
+// Sum of the valid squared errors of a lane's DPT datapoints in FP64: the
+// fallback when the FP32 Kahan sum overflowed (or a square is infinite); exact
+// for DPT finite squares and +Inf when one is infinite, like the reference's
+// double sum.  Out of line: it almost never runs.
+template <int DPT>
+__device__ __noinline__ double tile_sum_fp64(const float *T, const float *y, bool full,
+                                             int64_t dp0, int lane, int64_t N) {
+  double sum = 0.0;
+#pragma unroll
+  for (int k = 0; k < DPT; ++k) {
+    const bool valid = (full || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < N) && isfinite(T[k]);
+    const float df = __fsub_rn(T[k], y[k]);
+    sum += valid ? static_cast<double>(__fmul_rn(df, df)) : 0.0;
+  }
+  return sum;
 }
 
 // The producer thread of a block: claims work items (span, group) from the

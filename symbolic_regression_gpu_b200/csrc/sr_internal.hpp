@@ -83,11 +83,10 @@ SR_HD bool is_unary_token(int tok) {
 
 // Operator profiles of the interpreter: the set of opcodes its dispatch
 // switch handles inline (every other opcode goes through one out-of-line
-// routine, with identical results).  kOpsProtected: + - *, protected
-// division, sin, cos, exp clamped at 80, protected log and sqrt|x| (and their
-// reversed forms); kOpsAll: the arithmetic, divisions, roots, reciprocal,
-// sin / cos / exp / log families.  A launch uses kOpsProtected when at least
-// kProtectedShare of its instructions are in it.
+// routine, with identical results).  kOpsAll: every operator inline.
+// kOpsProtected: + - *, protected division, sin, cos, exp clamped at 80,
+// protected log and sqrt|x| (and their reversed forms).  A launch uses
+// kOpsProtected when at least kProtectedShare of its instructions are in it.
 constexpr int kOpsAll = 0;
 constexpr int kOpsProtected = 1;
 constexpr double kProtectedShare = 0.9;

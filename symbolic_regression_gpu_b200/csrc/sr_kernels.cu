@@ -43,7 +43,7 @@ namespace {
 
 // MAXW / MINB: launch bounds of the instantiation (at most MAXW evaluating
 // warps, at least MINB resident blocks per SM), which set the register budget.
-template <int DPT, bool PRED, int MAXW, int MINB, int OPS>
+template <int DPT, bool PRED, int MAXW, int MINB, int OPS, bool CACHE>
 __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const EvalArgs p) {
   constexpr int TILE = 32 * DPT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
         if (dp0 >= p.N) break;  // tail of the last span
         const float *xs = xb + t * TILE;
         float T[DPT];
-        run_program<DPT, OPS>(code, len, xs, span, st, lane, p.cache, p.ldc, dp0, T);
+        run_program<DPT, OPS, CACHE>(code, len, xs, span, st, lane, p.cache, p.ldc, dp0, T);
         if constexpr (PRED) {
           stg_vec<DPT>(p.pred + static_cast<int64_t>(p.pred_row[e]) * p.ldp + dp0, lane, T);
         } else {
@@ -130,17 +130,13 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
           }
           double tile_sum = static_cast<double>(s) - static_cast<double>(c);
           if (!isfinite(tile_sum)) {
-            // FP32 overflow of the running sum (or an infinite square): redo
-            // in FP64, which is exact for DPT finite squares and gives +Inf
-            // when one square is infinite, like the reference's double sum.
-            tile_sum = 0.0;
+            float tc[DPT], yc[DPT];
 #pragma unroll
             for (int k = 0; k < DPT; ++k) {
-              const bool valid =
-                  (full || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N) && isfinite(T[k]);
-              const float df = __fsub_rn(T[k], y[k]);
-              tile_sum += valid ? static_cast<double>(__fmul_rn(df, df)) : 0.0;
+              tc[k] = T[k];
+              yc[k] = y[k];
             }
+            tile_sum = tile_sum_fp64<DPT>(tc, yc, full, dp0, lane, p.N);
           }
           acc += tile_sum;
           cnt += nv;
@@ -298,40 +294,44 @@ size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span) {
          kBufs * sizeof(ItemDesc) + 2 * kBufs * sizeof(uint64_t);
 }
 
-template <int DPT, bool PRED, int MAXW, int MINB, int OPS = kOpsAll>
+template <int DPT, bool PRED, int MAXW, int MINB, int OPS = kOpsAll, bool CACHE = false>
 static const void *interp_fn() {
-  return reinterpret_cast<const void *>(&interp_kernel<DPT, PRED, MAXW, MINB, OPS>);
+  return reinterpret_cast<const void *>(&interp_kernel<DPT, PRED, MAXW, MINB, OPS, CACHE>);
 }
 
 template <int DPT, int MAXW, int MINB>
-static const void *interp_mse(int ops) {
-  return ops == kOpsProtected ? interp_fn<DPT, false, MAXW, MINB, kOpsProtected>()
-                              : interp_fn<DPT, false, MAXW, MINB, kOpsAll>();
+static const void *interp_mse(int ops, bool cache) {
+  if (cache)
+    return ops == kOpsProtected ? interp_fn<DPT, false, MAXW, MINB, kOpsProtected, true>()
+                                : interp_fn<DPT, false, MAXW, MINB, kOpsAll, true>();
+  return ops == kOpsProtected ? interp_fn<DPT, false, MAXW, MINB, kOpsProtected, false>()
+                              : interp_fn<DPT, false, MAXW, MINB, kOpsAll, false>();
 }
 
 // Instantiations: W <= 8 uses the narrow variants (more blocks per SM, tighter
 // register budget), larger W the wide ones.  MSE launches come in both
-// operator profiles, prediction launches in kOpsAll.
-static const void *select_interp(int dpt, bool pred, int ops, int W) {
+// operator profiles, with and without cached-subtree operands; prediction
+// launches (cache fills, predictions) in kOpsAll without.
+static const void *select_interp(int dpt, bool pred, int ops, bool cache, int W) {
   const bool narrow = W <= 8;
   if (dpt == 16) {
-    if (narrow) return pred ? interp_fn<16, true, 8, 2>() : interp_mse<16, 8, 2>(ops);
-    return pred ? interp_fn<16, true, 16, 1>() : interp_mse<16, 16, 1>(ops);
+    if (narrow) return pred ? interp_fn<16, true, 8, 2>() : interp_mse<16, 8, 2>(ops, cache);
+    return pred ? interp_fn<16, true, 16, 1>() : interp_mse<16, 16, 1>(ops, cache);
   }
   if (dpt == 8) {
-    if (narrow) return pred ? interp_fn<8, true, 8, 3>() : interp_mse<8, 8, 3>(ops);
-    return pred ? interp_fn<8, true, 16, 1>() : interp_mse<8, 16, 1>(ops);
+    if (narrow) return pred ? interp_fn<8, true, 8, 3>() : interp_mse<8, 8, 3>(ops, cache);
+    return pred ? interp_fn<8, true, 16, 1>() : interp_mse<8, 16, 1>(ops, cache);
   }
   if (dpt == 4) {
-    if (narrow) return pred ? interp_fn<4, true, 8, 4>() : interp_mse<4, 8, 4>(ops);
-    return pred ? interp_fn<4, true, 16, 2>() : interp_mse<4, 16, 2>(ops);
+    if (narrow) return pred ? interp_fn<4, true, 8, 4>() : interp_mse<4, 8, 4>(ops, cache);
+    return pred ? interp_fn<4, true, 16, 2>() : interp_mse<4, 16, 2>(ops, cache);
   }
   return nullptr;
 }
 
-cudaError_t interp_configure(int dpt, bool pred, int ops, size_t smem, int W,
+cudaError_t interp_configure(int dpt, bool pred, int ops, bool cache, size_t smem, int W,
                              int *blocks_per_sm) {
-  const void *fn = select_interp(dpt, pred, ops, W);
+  const void *fn = select_interp(dpt, pred, ops, cache, W);
   if (!fn || W < 1 || W > kMaxWarps) return cudaErrorInvalidValue;
   cudaError_t err = cudaFuncSetAttribute(
       fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -340,9 +340,9 @@ cudaError_t interp_configure(int dpt, bool pred, int ops, size_t smem, int W,
                                                        (W + 1) * 32, smem);
 }
 
-cudaError_t launch_interp(int dpt, bool pred, int ops, const EvalArgs &args, int blocks,
-                          size_t smem, cudaStream_t stream) {
-  const void *fn = select_interp(dpt, pred, ops, args.W);
+cudaError_t launch_interp(int dpt, bool pred, int ops, bool cache, const EvalArgs &args,
+                          int blocks, size_t smem, cudaStream_t stream) {
+  const void *fn = select_interp(dpt, pred, ops, cache, args.W);
   if (!fn || args.W < 1 || args.W > kMaxWarps) return cudaErrorInvalidValue;
   // Plans of one instantiation can differ in shared-memory size (main and
   // cache-fill sets, autotune candidates); the attribute belongs to the

@@ -19,12 +19,13 @@ size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span);
 // choice (deeper slots go to global scratch).
 inline int smem_spill_slots(int dpt) { return dpt >= 16 ? 2 : (dpt == 8 ? 4 : 8); }
 // Sets the dynamic-smem attribute and returns resident blocks per SM.
-// `ops` is the operator profile (kOpsAll / kOpsProtected, MSE mode only;
-// prediction launches always use kOpsAll).
-cudaError_t interp_configure(int dpt, bool pred, int ops, size_t smem, int W,
+// `ops` is the operator profile (kOpsAll / kOpsProtected) and `cache` whether
+// the programs read cached subtrees (MSE mode only; prediction launches use
+// kOpsAll without cached operands).
+cudaError_t interp_configure(int dpt, bool pred, int ops, bool cache, size_t smem, int W,
                              int *blocks_per_sm);
-cudaError_t launch_interp(int dpt, bool pred, int ops, const EvalArgs &args, int blocks,
-                          size_t smem, cudaStream_t stream);
+cudaError_t launch_interp(int dpt, bool pred, int ops, bool cache, const EvalArgs &args,
+                          int blocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_finalize(const double2 *partial, int n_spans, int E,
                             float *mse, cudaStream_t stream);
 cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *off,
