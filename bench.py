@@ -196,10 +196,12 @@ def cpu_baseline(w, target_s: float, threads: int):
     n = int(max(threads, min(E, tokens_target / mean_len)))
     sample = pop.subset(order[:n])
     t0 = time.perf_counter()
-    oracle.ref_mse(sample, w.X, threads=threads)
+    ref = oracle.ref_mse(sample, w.X, threads=threads)
     dt = time.perf_counter() - t0
     value = sample.num_tokens * w.num_dps / dt
+    ref_mse = np.asarray(ref[0] if isinstance(ref, tuple) else ref, np.float32)
     return {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+            "_sample_index": order[:n], "_sample_mse": ref_mse,
             "sample": f"{n} of {E} expressions (seeded subset) x all {w.num_dps} datapoints, "
                       f"{dt:.1f} s; reference evaluate_cpu_mse (src/cleaned/cl_cpu_eval.cpp) "
                       f"compiled -O3, THREADS={threads}; exp_clamp80 timed as the reference "
@@ -513,6 +515,20 @@ def run_ours(args):
         except (OSError, ValueError):
             traffic = None
 
+    # Accuracy of the timed results: every expression's MSE against its FP64
+    # reference, evaluated on the device (outside the timed region).
+    accuracy = None
+    if rank == 0:
+        rel = ev.accuracy(w.population, mse)
+        fin = rel[np.isfinite(rel)]
+        accuracy = {"reference": "FP64 evaluation on the device (sr_eval_mse_fp64)",
+                    "expressions": int(w.population.num_exprs), "finite": int(fin.size),
+                    "median_rel_err": float(np.median(fin)) if fin.size else None,
+                    "p99_rel_err": float(np.quantile(fin, 0.99)) if fin.size else None,
+                    "frac_le_1e-5": float(np.mean(fin <= 1e-5)) if fin.size else None,
+                    "frac_le_1e-6": float(np.mean(fin <= 1e-6)) if fin.size else None}
+        ev.prepare(w.population)
+
     # Plain per-expression kernel on the same population (baseline ratio).
     plain = None
     if args.plain_baseline and rank == 0:
@@ -578,6 +594,24 @@ def run_ours(args):
             cpu = cpu_baseline(w, args.cpu_seconds, os.cpu_count() or 1)
         except (ImportError, FileNotFoundError, OSError) as ex:
             cpu = {"value": None, "unavailable": str(ex)}
+        if cpu.get("_sample_index") is not None:
+            # The reference's FP32 results on the sample against the same FP64
+            # reference, beside ours on the same expressions.
+            idx = cpu.pop("_sample_index")
+            ref_mse = cpu.pop("_sample_mse")
+            sample = w.population.subset(idx)
+            ev.set_data(w.X)
+            mse64 = ev.eval_mse_fp64(sample)
+
+            def _stats(m):
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    r = np.abs(np.asarray(m, np.float64) - mse64) / np.maximum(np.abs(mse64), 1e-300)
+                r = r[np.isfinite(r)]
+                return {"median_rel_err": float(np.median(r)) if r.size else None,
+                        "frac_le_1e-5": float(np.mean(r <= 1e-5)) if r.size else None,
+                        "finite": int(r.size)}
+            cpu["accuracy_vs_fp64"] = {"reference_cpu": _stats(ref_mse),
+                                       "this_gpu_same_expressions": _stats(mse[idx])}
 
     if rank == 0:
         line = {
@@ -611,6 +645,7 @@ def run_ours(args):
             "device_evolution": evolution,
             "large": large,
             "mse_finite": int(np.isfinite(mse).sum()),
+            "accuracy_vs_fp64": accuracy,
         }
         print(json.dumps(line))
     ev.close()

@@ -358,6 +358,14 @@ sr_status sr_eval_mse_device_noalloc(const int32_t *tokens, const float *values,
                                      float *mse_out, void *stream);
 
 /* ---- misc ------------------------------------------------------------------ */
+/* FP64 reference MSE of every expression, evaluated on the device: the same
+ * operators in double, constants as (double)(float)value, the FP32 dataset,
+ * a datapoint counted when its FP64 prediction would be a finite float.
+ * The accuracy report of the FP32 results: |mse - mse_fp64| / |mse_fp64|
+ * per expression.  No reference counterpart (the reference reports FP32
+ * results only).  Synchronous; clears the prepared launch. */
+sr_status sr_eval_mse_fp64(sr_context *ctx, const sr_population *pop, double *mse64_out);
+
 /* ---- the generation loop on the device ---------------------------------------
  * The reference runs its evolution loop on the host (src/cleaned/cl_sr_system.cpp:
  * 150-330: evaluate, sort by fitness with NaN last, keep the top 5 %, fill the rest

@@ -190,6 +190,7 @@ _SIGNATURES = {
                                         _P(c_int64), _P(c_int32)]),
     "sr_eval_mse_device_noalloc": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                              c_int64, c_int32, c_int64, c_void_p, c_void_p]),
+    "sr_eval_mse_fp64": (c_int32, [c_void_p, _P(sr_population), _P(c_double)]),
     "sr_evolve_options_init": (c_int32, [_P(sr_evolve_options), c_int32]),
     "sr_evolve_init": (c_int32, [c_void_p, _P(sr_evolve_options), c_int32, c_int32, c_void_p,
                                  c_void_p, c_void_p]),

@@ -35,8 +35,22 @@ double now_ms() {
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Milliseconds between two events, 0 when either was never recorded (the
+// device-resident paths skip the upload pair).  cudaEventElapsedTime reports
+// that case as an error that would otherwise stay as the thread's last error
+// and surface at the next launch check, so it is consumed here.
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.f;
+  }
+  return ms;
+}
+
 sr_status cuda_fail(sr_context *ctx, cudaError_t e, const char *what) {
   const sr_status s = (e == cudaErrorMemoryAllocation) ? SR_ERR_OUT_OF_MEMORY : SR_ERR_CUDA;
+  cudaGetLastError();  // reported here; a non-sticky error must not fail the next call's launch check
   return ctx->fail(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -363,8 +377,7 @@ sr_status autotune_main(sr_context *ctx, const std::string &key) {
       SR_TRY(launch_set(ctx, ctx->main, false, ctx->d_counter, nullptr, 0, nullptr));
       SR_TRY_CUDA(ctx, cudaEventRecord(b, ctx->stream));
       SR_TRY_CUDA(ctx, cudaEventSynchronize(b));
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, a, b);
+      const float ms = elapsed_ms(a, b);
       if (rep > 0) t_sum += ms;  // first run warms up
     }
     if (t_sum < best) {
@@ -1017,13 +1030,9 @@ static void fill_stats(sr_context *ctx, sr_stats *st) {
   if (!st) return;
   *st = ctx->prep_stats;
   if (ctx->timing_valid) {
-    float k = 0.f, ev = 0.f, up = 0.f;
-    cudaEventElapsedTime(&k, ctx->ev[0], ctx->ev[3]);
-    cudaEventElapsedTime(&ev, ctx->ev[1], ctx->ev[2]);
-    cudaEventElapsedTime(&up, ctx->ev[4], ctx->ev[5]);
-    st->gpu_kernel_time_ms = k;
-    st->eval_kernel_time_ms = ev;
-    st->data_transfer_time_ms = up;
+    st->gpu_kernel_time_ms = elapsed_ms(ctx->ev[0], ctx->ev[3]);
+    st->eval_kernel_time_ms = elapsed_ms(ctx->ev[1], ctx->ev[2]);
+    st->data_transfer_time_ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
   }
   if (ctx->mode == sr::Mode::kBatched || ctx->mode == sr::Mode::kCached) {
     st->declared_sfu_ops = ctx->main.sfu_per_dp * static_cast<double>(ctx->N);
@@ -1507,6 +1516,45 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
   return SR_OK;
 }
 
+sr_status sr_eval_mse_fp64(sr_context *ctx, const sr_population *pop, double *mse64_out) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  ctx->last_error.clear();
+  SR_TRY(check_population(ctx, pop));
+  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
+  const int E = pop->num_exprs;
+  if (E == 0) return SR_OK;
+  if (!mse64_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "mse64_out is NULL");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  reset_prepared(ctx);
+  ctx->prep_stats = sr_stats{};
+  for (int x = 0; x < E; ++x) {  // the FP64 kernel's stack is shallower than the plain one's
+    int depth = 0, maxd = 0;
+    for (int64_t i = pop->offsets[x + 1] - 1; i >= pop->offsets[x]; --i) {
+      const int t = pop->tokens[i];
+      if (t <= 0) ++depth;
+      else if (sr::is_binary_token(t)) --depth;
+      maxd = std::max(maxd, depth);
+    }
+    if (maxd > sr::kFp64Stack)
+      return ctx->fail(SR_ERR_UNSUPPORTED, "expression " + std::to_string(x) +
+                                               " is deeper than the FP64 reference stack (" +
+                                               std::to_string(sr::kFp64Stack) + ")");
+  }
+  SR_TRY(prepare_plain(ctx, pop));  // raw tokens on the device, as the plain kernel reads them
+  SR_TRY_CUDA(ctx, ctx->mse64.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->h_mse64.ensure(static_cast<size_t>(E)));
+  sr::PlainSet &ps = ctx->plain;
+  SR_TRY_CUDA(ctx, sr::launch_fp64(ps.tok.p, ps.val.p, ps.off.p, ps.len.p, ctx->X.p, ctx->ldx,
+                                   ctx->V, ctx->N, E, ctx->partial.p, ps.n_dpblocks,
+                                   ctx->mse64.p, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_mse64.p, ctx->mse64.p, E * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(mse64_out, ctx->h_mse64.p, E * sizeof(double));
+  return SR_OK;
+}
+
 // ---- the generation loop on the device ------------------------------------------
 
 sr_status sr_evolve_options_init(sr_evolve_options *o, int32_t num_vars) {
@@ -1737,8 +1785,7 @@ sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s, double *sfu_
         cudaFree(dummy);
         return cuda_fail(ctx, e != cudaSuccess ? e : cudaGetLastError(), "pipe benchmark");
       }
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+      const float ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
       if (rep > 0) best = std::min(best, ms);
     }
     rates[m] = static_cast<double>(blocks) * threads * iters * 8.0 / (best * 1e-3);

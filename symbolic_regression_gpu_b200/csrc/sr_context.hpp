@@ -227,6 +227,9 @@ struct sr_context {
   sr::DevBuf<float> spill;
   // gradients / constant optimisation
   sr::GradSet grad;
+  // FP64 accuracy report
+  sr::DevBuf<double> mse64;
+  sr::PinnedBuf<double> h_mse64;
   // device common-subtree detection
   sr::DetectBufs det;
   // device-side evolution: ranking scratch and the device-compile summary

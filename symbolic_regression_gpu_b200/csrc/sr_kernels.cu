@@ -20,6 +20,8 @@
 //                             or stores the predictions.
 //  finalize_kernel            per-expression combination of span partials in
 //                             a fixed order: mse = sum / count.
+//  fp64_kernel                the plain kernel's shape in double: the FP64
+//                             reference of the accuracy report.
 //  plain_kernel               baseline with the reference's launch shape
 //                             (4 expressions x 128 datapoints per block, token
 //                             stack in local memory), fused MSE reduction.
@@ -254,6 +256,93 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// FP64 reference evaluation for the accuracy report: the plain kernel's
+// shape with every operator in double, constants entering as (double)(float)
+// value and the variables as the FP32 dataset; a datapoint counts when its
+// FP64 prediction would be a finite float (the FP32 path's validity rule).
+__global__ void __launch_bounds__(128)
+    fp64_kernel(const int32_t *__restrict__ tok, const float *__restrict__ val,
+                const int64_t *__restrict__ off, const int32_t *__restrict__ len,
+                const float *__restrict__ X, int64_t ldx, int V, int64_t N, int E,
+                double2 *__restrict__ partial) {
+  __shared__ double red_s[4][4];
+  __shared__ int red_c[4][4];
+  const int e0 = blockIdx.x * 4;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  int cnt[4] = {0, 0, 0, 0};
+  for (int64_t dp = static_cast<int64_t>(blockIdx.y) * 128 + threadIdx.x; dp < N;
+       dp += static_cast<int64_t>(gridDim.y) * 128) {
+    const double yv = static_cast<double>(X[V * ldx + dp]);
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j) {
+      const int e = e0 + j;
+      if (e >= E) break;
+      double stk[kFp64Stack];  // the frame stays below the default stack limit
+      int sp = 0;
+      const int64_t o = off[e];
+      for (int i = len[e] - 1; i >= 0; --i) {
+        const int t = tok[o + i];
+        if (t > 0) {
+          const double v1 = stk[--sp];
+          double v2 = 0.0;
+          if (t < 10) v2 = stk[--sp];
+          stk[sp++] = op_apply_f64(t, v1, v2);
+        } else if (t == 0) {
+          stk[sp++] = static_cast<double>(val[o + i]);
+        } else {
+          const int vi = static_cast<int>(val[o + i]);
+          stk[sp++] = (vi >= 0 && vi < V) ? static_cast<double>(X[vi * ldx + dp]) : 0.0;
+        }
+      }
+      const double pred = stk[0];
+      if (!isnan(pred) && !isinf(static_cast<float>(pred))) {
+        const double d = pred - yv;
+        acc[j] += d * d;
+        cnt[j] += 1;
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double s = acc[j];
+    int c = cnt[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+      red_s[j][warp] = s;
+      red_c[j][warp] = c;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int j = threadIdx.x;
+    const int e = e0 + j;
+    if (e < E) {
+      const double s = red_s[j][0] + red_s[j][1] + red_s[j][2] + red_s[j][3];
+      const int c = red_c[j][0] + red_c[j][1] + red_c[j][2] + red_c[j][3];
+      partial[static_cast<int64_t>(blockIdx.y) * E + e] =
+          make_double2(s, static_cast<double>(c));
+    }
+  }
+}
+
+__global__ void finalize_f64_kernel(const double2 *__restrict__ partial, int n_spans, int E,
+                                    double *__restrict__ mse) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  double s = 0.0, c = 0.0;
+  for (int k = 0; k < n_spans; ++k) {
+    const double2 q = partial[static_cast<int64_t>(k) * E + e];
+    s += q.x;
+    c += q.y;
+  }
+  mse[e] = (c > 0.0) ? s / c : __longlong_as_double(0x7ff8000000000000ll);
+}
+
 // ---- pipe microbenchmarks (8 independent chains per thread) ----
 __global__ void fma_pipe_kernel(float *out, int iters) {
   float r[8];
@@ -369,6 +458,21 @@ cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *of
   const dim3 grid((E + 3) / 4, n_dpblocks);
   plain_kernel<<<grid, 128, 0, stream>>>(tok, val, off, len, X, ldx, V, N, E,
                                          partial);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fp64(const int32_t *tok, const float *val, const int64_t *off,
+                       const int32_t *len, const float *X, int64_t ldx, int V, int64_t N, int E,
+                       double2 *partial, int n_dpblocks, double *mse64, cudaStream_t stream) {
+  if (E <= 0) return cudaSuccess;
+  if (n_dpblocks > 0 && N > 0) {
+    const dim3 grid((E + 3) / 4, n_dpblocks);
+    fp64_kernel<<<grid, 128, 0, stream>>>(tok, val, off, len, X, ldx, V, N, E, partial);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+  }
+  finalize_f64_kernel<<<(E + 255) / 256, 256, 0, stream>>>(partial, N > 0 ? n_dpblocks : 0, E,
+                                                           mse64);
   return cudaGetLastError();
 }
 

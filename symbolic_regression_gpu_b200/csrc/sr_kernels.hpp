@@ -12,6 +12,7 @@ constexpr int kMaxWarps = 16;                       // evaluating warps per bloc
 constexpr int kMaxBlockThreads = (kMaxWarps + 1) * 32;  // + producer warp
 constexpr int64_t kDataAlign = 4096;               // X / cache row stride multiple
 constexpr int kPlainStack = 128;                    // plain kernel stack depth
+constexpr int kFp64Stack = 96;                      // FP64 reference kernel stack depth
 
 // Dynamic shared memory of interp_kernel for a launch shape.
 size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span);
@@ -32,6 +33,10 @@ cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *of
                          const int32_t *len, const float *X, int64_t ldx, int V,
                          int64_t N, int E, double2 *partial, int n_dpblocks,
                          cudaStream_t stream);
+// FP64 evaluation of the plain set (accuracy report): mse64[e] in double.
+cudaError_t launch_fp64(const int32_t *tok, const float *val, const int64_t *off,
+                       const int32_t *len, const float *X, int64_t ldx, int V, int64_t N, int E,
+                       double2 *partial, int n_dpblocks, double *mse64, cudaStream_t stream);
 cudaError_t launch_pipe_bench(bool mufu, float *out, int blocks, int threads,
                               int iters, cudaStream_t stream);
 

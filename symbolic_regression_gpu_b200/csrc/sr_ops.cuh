@@ -66,4 +66,42 @@ __device__ __forceinline__ float op_apply(int op, float x, float y) {
   return (op >= 1 && op <= 9) ? op_binary(op, x, y) : op_unary(op, x);
 }
 
+// The same operators evaluated in double: the FP64 reference of the accuracy
+// report (MIN / MAX as fmin / fmax like the float path; the protected regions
+// at 1e-9; LOOSE_LOG -1e9 at 0).
+__device__ __forceinline__ double op_apply_f64(int op, double x, double y) {
+  const double kDelta = 1e-9;
+  switch (op) {
+    case 1: return x + y;
+    case 2: return x - y;
+    case 3: return x * y;
+    case 4: return (y == 0.0) ? __longlong_as_double(0x7ff8000000000000ll) : x / y;
+    case 5: return pow(x, y);
+    case 6: return fmin(x, y);
+    case 7: return fmax(x, y);
+    case 8: return x / (fabs(y) <= kDelta ? (y < 0.0 ? -kDelta : kDelta) : y);
+    case 9: return (x == 0.0 && y == 0.0) ? 0.0 : pow(fabs(x), y);
+    case 10: return sin(x);
+    case 11: return cos(x);
+    case 12: return tan(x);
+    case 13: return sinh(x);
+    case 14: return cosh(x);
+    case 15: return tanh(x);
+    case 16: return exp(x);
+    case 17: return log(x);
+    case 18: return 1.0 / x;
+    case 19: return asin(x);
+    case 20: return acos(x);
+    case 21: return atan(x);
+    case 22: return (x == 0.0) ? -1e9 : log(fabs(x));
+    case 23: return 1.0 / (fabs(x) <= kDelta ? (x < 0.0 ? -kDelta : kDelta) : x);
+    case 24: return fabs(x);
+    case 25: return -x;
+    case 26: return sqrt(x);
+    case 27: return sqrt(fabs(x));
+    case 32: return exp(fmin(x, 80.0));
+    default: return 0.0;
+  }
+}
+
 }  // namespace sr

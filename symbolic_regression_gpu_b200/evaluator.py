@@ -134,6 +134,26 @@ class Evaluator:
                                          ctypes.byref(self.stats)), "sr_eval_mse")
         return out
 
+    def eval_mse_fp64(self, pop: Population) -> np.ndarray:
+        """FP64 reference MSE of every expression, evaluated on the GPU (the
+        accuracy report of the FP32 results; float64 [E])."""
+        out = np.empty(pop.num_exprs, np.float64)
+        cpop = pop.as_c()
+        self._check(_lib.lib.sr_eval_mse_fp64(self._ctx, ctypes.byref(cpop),
+                                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                    "sr_eval_mse_fp64")
+        return out
+
+    def accuracy(self, pop: Population, mse: np.ndarray) -> np.ndarray:
+        """|mse - mse_fp64| / |mse_fp64| per expression (NaN where either is
+        not finite)."""
+        ref = self.eval_mse_fp64(pop)
+        m = np.asarray(mse, np.float64)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            rel = np.abs(m - ref) / np.maximum(np.abs(ref), 1e-300)
+        rel[~(np.isfinite(m) & np.isfinite(ref))] = np.nan
+        return rel
+
     def prepare(self, pop: Population, *, cache: bool = False, clear_cache: bool = False,
                 plain: bool = False, gradient: bool = False,
                 grad_mode: int = _lib.SR_GRAD_CHECKPOINT):

@@ -107,6 +107,10 @@ def test_device_compile_matches_host_compile(data):
         de.evaluate()
         got = de.fitness()
         st = ev.stats
+        # The device-resident evaluation records no upload events; reading its
+        # stats must leave no CUDA error behind for the next call's launches.
+        mse64 = ev.eval_mse_fp64(pop.subset(np.arange(8)))
+    assert np.isfinite(mse64).any()
     same = (got.view(np.uint32) == want32.view(np.uint32)) | (np.isnan(got) & np.isnan(want32))
     assert same.all()
     assert st.node_evals == pop.num_tokens * w.num_dps
