@@ -177,6 +177,55 @@ def _reference_population(pop):
     return Population(tok, pop.values, pop.offsets)
 
 
+def _ulp_distance(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Distance in representable floats between FP32 arrays (0 for two NaNs,
+    a large value when exactly one is NaN)."""
+    def ordered(x):
+        i = np.asarray(x, np.float32).view(np.int32).astype(np.int64)
+        return np.where(i < 0, -(i & 0x7FFFFFFF), i)
+    d = np.abs(ordered(a) - ordered(b))
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.where(na & nb, 0, np.where(na | nb, 1 << 40, d))
+
+
+def parity_figures(ev, w, sample, ours_mse, ref_mse):
+    """Parity of the GPU path against the reference on the CPU-baseline sample:
+    MSE against the reference's evaluate_cpu_mse, per-datapoint ulp against the
+    reference's per-datapoint evaluation (the oracle's predict_f32, pinned bit
+    for bit to evaluate_single_expr) on sampled datapoints, and the reduction
+    error alone (our MSE against an FP64 sum of our own FP32 predictions)."""
+    from oracle import oracle
+    out = {}
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r = np.abs(np.asarray(ours_mse, np.float64) - ref_mse) / np.maximum(np.abs(ref_mse), 1e-300)
+    both = np.isfinite(ours_mse) & np.isfinite(ref_mse)
+    out["mse_vs_reference_cpu"] = {
+        "expressions": int(both.sum()),
+        "median_rel": float(np.median(r[both])) if both.any() else None,
+        "frac_le_1e-6": float(np.mean(r[both] <= 1e-6)) if both.any() else None,
+        "nan_pattern_equal": bool(np.array_equal(np.isnan(ours_mse), np.isnan(ref_mse)))}
+    ns = min(4096, w.num_dps)
+    sub = sample.subset(np.arange(min(512, sample.num_exprs)))
+    ours = ev.predictions(sub, 0, ns)
+    theirs = oracle.predict_f32(sub, np.ascontiguousarray(w.X[:, :ns]))
+    u = _ulp_distance(ours, theirs)
+    out["per_datapoint_ulp"] = {
+        "expressions": int(sub.num_exprs), "datapoints": int(ns),
+        "bit_identical": float(np.mean(u == 0)), "frac_le_4ulp": float(np.mean(u <= 4)),
+        "violations_gt_4ulp": int(np.count_nonzero(u > 4))}
+    red = sample.subset(np.arange(min(16, sample.num_exprs)))
+    pred = ev.predictions(red)
+    sums = oracle.mse_of_predictions(pred, w.X[w.num_vars])
+    del pred
+    ours_red = np.asarray(ours_mse[:red.num_exprs], np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rr = np.abs(ours_red - sums) / np.maximum(np.abs(sums), 1e-300)
+    rr = rr[np.isfinite(rr)]
+    out["reduction_error"] = {"expressions": int(red.num_exprs),
+                              "max_rel": float(rr.max()) if rr.size else None}
+    return out
+
+
 def cpu_baseline(w, target_s: float, threads: int):
     """Reference evaluate_cpu_mse (oracle/_ref, compiled -O3) on a seeded
     expression subset over the full datapoint range."""
@@ -612,6 +661,7 @@ def run_ours(args):
                         "finite": int(r.size)}
             cpu["accuracy_vs_fp64"] = {"reference_cpu": _stats(ref_mse),
                                        "this_gpu_same_expressions": _stats(mse[idx])}
+            cpu["parity"] = parity_figures(ev, w, sample, mse[idx], ref_mse)
 
     if rank == 0:
         line = {

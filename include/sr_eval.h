@@ -215,6 +215,14 @@ sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats);
 sr_status sr_last_launch_times(sr_context *ctx, float *launch_ms, float *eval_kernel_ms);
 /* Device pointer of the MSE vector written by sr_launch (num_exprs floats). */
 sr_status sr_device_mse(sr_context *ctx, float **mse_dev);
+/* Datapoint sharding: after sr_launch (or sr_eval_mse / sr_eval_grad), the
+ * FP64 sum of the valid squared errors and the valid-datapoint count of every
+ * expression (sum_out[i] / count_out[i] is the MSE before its rounding to
+ * float; count 0 = no valid datapoint).  A caller that splits the datapoints
+ * over several contexts (one per GPU, each holding its columns of X) adds the
+ * shards' sums and counts and divides.  No reference counterpart (the
+ * reference evaluates every datapoint on one GPU, cl_gpu_eval.cu:332-564). */
+sr_status sr_read_sums(sr_context *ctx, double *sum_out, double *count_out);
 
 /* Per-datapoint predictions of every expression for dps [dp_begin,
  * dp_begin+dp_count): pred_out[i * dp_count + j].  Predictions are the raw
@@ -247,6 +255,10 @@ sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode,
 /* After sr_prepare(..., SR_EVAL_GRADIENT) and sr_launch: the gradient of the
  * last launch (CSR layout above); sr_read_mse gives its MSE. */
 sr_status sr_read_grad(sr_context *ctx, float *grad_out);
+/* Datapoint sharding of the gradient: the FP64 sum over valid datapoints of
+ * d (squared error) / d constant (CSR layout above); the gradient is this sum
+ * divided by the expression's valid count (sr_read_sums). */
+sr_status sr_read_grad_sums(sr_context *ctx, double *grad_sum_out);
 
 /* On-device Adam over every expression's constants (steps iterations of
  * fused forward+adjoint then an Adam update); const_out receives the final

@@ -166,6 +166,8 @@ _SIGNATURES = {
     "sr_launch": (c_int32, [c_void_p]),
     "sr_read_mse": (c_int32, [c_void_p, _P(c_float), _P(sr_stats)]),
     "sr_read_grad": (c_int32, [c_void_p, _P(c_float)]),
+    "sr_read_sums": (c_int32, [c_void_p, _P(c_double), _P(c_double)]),
+    "sr_read_grad_sums": (c_int32, [c_void_p, _P(c_double)]),
     "sr_device_mse": (c_int32, [c_void_p, _P(c_void_p)]),
     "sr_last_launch_times": (c_int32, [c_void_p, _P(c_float), _P(c_float)]),
     "sr_eval_predictions": (c_int32, [c_void_p, _P(sr_population), c_int64, c_int64, _P(c_float)]),

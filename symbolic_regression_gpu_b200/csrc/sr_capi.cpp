@@ -1063,6 +1063,52 @@ sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats) {
   return SR_OK;
 }
 
+sr_status sr_read_sums(sr_context *ctx, double *sum_out, double *count_out) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (ctx->E == 0) return SR_OK;
+  if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing launched");
+  if (!sum_out || !count_out)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "sum_out / count_out is NULL");
+  int n_spans = 0;
+  switch (ctx->mode) {
+    case sr::Mode::kPlain: n_spans = ctx->N > 0 ? ctx->plain.n_dpblocks : 0; break;
+    case sr::Mode::kGrad: n_spans = ctx->grad.n_spans; break;
+    default: n_spans = ctx->main.plan.n_spans; break;
+  }
+  const int E = ctx->E;
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the buffers may grow
+  SR_TRY_CUDA(ctx, ctx->sums.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, ctx->h_sums.ensure(static_cast<size_t>(E)));
+  SR_TRY_CUDA(ctx, sr::launch_sums(ctx->partial.p, n_spans, E, ctx->sums.p, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_sums.p, ctx->sums.p, E * sizeof(double2),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  SR_TRY(check_device_error(ctx));
+  for (int e = 0; e < E; ++e) {
+    sum_out[e] = ctx->h_sums.p[e].x;
+    count_out[e] = ctx->h_sums.p[e].y;
+  }
+  return SR_OK;
+}
+
+sr_status sr_read_grad_sums(sr_context *ctx, double *grad_sum_out) {
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (ctx->E == 0) return SR_OK;
+  if (ctx->mode != sr::Mode::kGrad)
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "no gradient prepared (SR_EVAL_GRADIENT)");
+  const int64_t C = ctx->grad.C;
+  if (C == 0) return SR_OK;
+  if (!grad_sum_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "grad_sum_out is NULL");
+  DeviceScope scope(ctx->device);
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(grad_sum_out, ctx->grad.grad_acc.p, C * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SR_OK;
+}
+
 sr_status sr_read_grad(sr_context *ctx, float *grad_out) {
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (ctx->E == 0) return SR_OK;

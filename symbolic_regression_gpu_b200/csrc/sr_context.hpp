@@ -230,6 +230,8 @@ struct sr_context {
   // FP64 accuracy report
   sr::DevBuf<double> mse64;
   sr::PinnedBuf<double> h_mse64;
+  sr::DevBuf<double2> sums;  // (sum, count) per expression for datapoint sharding
+  sr::PinnedBuf<double2> h_sums;
   // device common-subtree detection
   sr::DetectBufs det;
   // device-side evolution: ranking scratch and the device-compile summary

@@ -20,6 +20,8 @@
 //                             or stores the predictions.
 //  finalize_kernel            per-expression combination of span partials in
 //                             a fixed order: mse = sum / count.
+//  sums_kernel                the same combination kept as (sum, count), for
+//                             datapoint-sharded callers.
 //  fp64_kernel                the plain kernel's shape in double: the FP64
 //                             reference of the accuracy report.
 //  plain_kernel               baseline with the reference's launch shape
@@ -177,6 +179,21 @@ __global__ void finalize_kernel(const double2 *__restrict__ partial, int n_spans
   // Reference: mses[i] = total_sq_err / valid_dps, or NaN when no datapoint
   // is valid (src/cleaned/cl_cpu_eval.cpp:154-158).
   mse[e] = (c > 0.0) ? static_cast<float>(s / c) : qnan();
+}
+
+// The same fixed-order combination as finalize_kernel, kept as (sum, count)
+// for callers that add the partial sums of several datapoint shards.
+__global__ void sums_kernel(const double2 *__restrict__ partial, int n_spans, int E,
+                            double2 *__restrict__ sums) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  double s = 0.0, c = 0.0;
+  for (int k = 0; k < n_spans; ++k) {
+    const double2 q = partial[static_cast<int64_t>(k) * E + e];
+    s += q.x;
+    c += q.y;
+  }
+  sums[e] = make_double2(s, c);
 }
 
 // Plain baseline: the reference launch shape (4 expressions x 128 datapoints
@@ -473,6 +490,13 @@ cudaError_t launch_fp64(const int32_t *tok, const float *val, const int64_t *off
   }
   finalize_f64_kernel<<<(E + 255) / 256, 256, 0, stream>>>(partial, N > 0 ? n_dpblocks : 0, E,
                                                            mse64);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sums(const double2 *partial, int n_spans, int E, double2 *sums,
+                        cudaStream_t stream) {
+  if (E <= 0) return cudaSuccess;
+  sums_kernel<<<(E + 255) / 256, 256, 0, stream>>>(partial, n_spans, E, sums);
   return cudaGetLastError();
 }
 

@@ -29,6 +29,10 @@ cudaError_t launch_interp(int dpt, bool pred, int ops, bool cache, const EvalArg
                           int blocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_finalize(const double2 *partial, int n_spans, int E,
                             float *mse, cudaStream_t stream);
+// (sum of valid squared errors, valid count) per expression, combined over
+// the span partials in the order launch_finalize uses.
+cudaError_t launch_sums(const double2 *partial, int n_spans, int E, double2 *sums,
+                        cudaStream_t stream);
 cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *off,
                          const int32_t *len, const float *X, int64_t ldx, int V,
                          int64_t N, int E, double2 *partial, int n_dpblocks,

@@ -132,6 +132,7 @@ class Evaluator:
         self._check(_lib.lib.sr_eval_mse(self._ctx, ctypes.byref(cpop),
                                          self._flags(cache, clear_cache, plain), _f32ptr(out),
                                          ctypes.byref(self.stats)), "sr_eval_mse")
+        self._E = pop.num_exprs
         return out
 
     def eval_mse_fp64(self, pop: Population) -> np.ndarray:
@@ -185,6 +186,30 @@ class Evaluator:
         self._check(_lib.lib.sr_read_grad(self._ctx, _f32ptr(out)), "sr_read_grad")
         return out[:self._C]
 
+    def read_sums(self):
+        """(FP64 sum of valid squared errors [E], valid count [E]) of the last
+        launch: the partial result a datapoint shard contributes."""
+        sums = np.empty(max(self._E, 1), np.float64)
+        cnt = np.empty(max(self._E, 1), np.float64)
+        P = ctypes.POINTER(ctypes.c_double)
+        self._check(_lib.lib.sr_read_sums(self._ctx, sums.ctypes.data_as(P),
+                                          cnt.ctypes.data_as(P)), "sr_read_sums")
+        return sums[:self._E], cnt[:self._E]
+
+    def read_grad_sums(self) -> np.ndarray:
+        """FP64 sum over valid datapoints of d (squared error) / d constant, of
+        the last gradient launch (CSR over expressions)."""
+        out = np.empty(max(self._C, 1), np.float64)
+        self._check(_lib.lib.sr_read_grad_sums(
+            self._ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "sr_read_grad_sums")
+        return out[:self._C]
+
+    def eval_sums(self, pop: Population):
+        """Batched evaluation of `pop` on this context's datapoints, returning
+        read_sums() (the datapoint-shard contribution)."""
+        self.eval_mse(pop)
+        return self.read_sums()
+
     def last_launch_times(self):
         """(whole launch ms, main interpreter kernel ms) of the last launch."""
         a = ctypes.c_float()
@@ -218,6 +243,7 @@ class Evaluator:
         self._check(_lib.lib.sr_eval_grad(self._ctx, ctypes.byref(cpop), mode, _f32ptr(mse),
                                           _f32ptr(grad), ctypes.byref(self.stats)),
                     "sr_eval_grad")
+        self._E, self._C = pop.num_exprs, nconst
         return mse, grad[:nconst]
 
     def optimize_constants(self, pop: Population, steps: int = 20, lr: float = 0.05,

@@ -53,6 +53,12 @@ class Population:
     def lengths(self) -> np.ndarray:
         return np.diff(self.offsets)
 
+    def constant_counts(self) -> np.ndarray:
+        """Constant tokens (TOK_CONST) per expression: the CSR row lengths of
+        the gradient layout."""
+        is_c = np.concatenate(([0], np.cumsum(self.tokens == 0, dtype=np.int64)))
+        return np.diff(is_c[self.offsets])
+
     def expr(self, i: int) -> Tuple[np.ndarray, np.ndarray]:
         a, b = int(self.offsets[i]), int(self.offsets[i + 1])
         return self.tokens[a:b], self.values[a:b]

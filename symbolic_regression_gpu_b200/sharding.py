@@ -14,6 +14,14 @@ The reference evaluates on one GPU only (src/cleaned/cl_gpu_eval.cu:332-564);
 this module is the multi-GPU partition of the same call.  Slices are
 contiguous in population order, so the gathered vector is the concatenation
 of the slices and needs no permutation.
+
+Datapoint sharding (DatapointShardedEvaluator) is the partition for datasets
+larger than one GPU's memory: rank r keeps only the columns [d[r], d[r+1]) of
+X and evaluates the whole population on them; every rank then all-gathers the
+per-expression FP64 (sum of valid squared errors, valid count) pairs (16 bytes
+per expression per rank) and adds them in rank order, so the result is the
+same on every rank and from run to run.  Gradients combine the same way
+(FP64 gradient sums over the valid datapoints, divided by the total count).
 """
 from __future__ import annotations
 
@@ -148,3 +156,135 @@ class ShardedEvaluator:
 def split_counts(bounds: np.ndarray) -> List[int]:
     """Expressions per rank of a bounds vector."""
     return [int(x) for x in np.diff(bounds)]
+
+
+def datapoint_bounds(num_dps: int, world: int, align: int = 1024) -> np.ndarray:
+    """Boundaries d[0]=0 <= ... <= d[world]=num_dps of contiguous datapoint
+    shards of about equal size, interior boundaries on multiples of `align`
+    (a whole number of the evaluator's datapoint spans)."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    if num_dps < 0:
+        raise ValueError("negative datapoint count")
+    d = np.empty(world + 1, dtype=np.int64)
+    d[0], d[world] = 0, num_dps
+    for r in range(1, world):
+        cut = (num_dps * r) // world
+        d[r] = min(num_dps, ((cut + align // 2) // align) * align)
+    np.maximum.accumulate(d, out=d)
+    return d
+
+
+def combine_sums(sums: np.ndarray, counts: np.ndarray) -> np.ndarray:
+    """MSE from per-rank sums and counts [world, E], added in rank order (FP64)
+    and divided as the single-GPU finalisation does: float32(sum / count), NaN
+    where no datapoint of any shard is valid."""
+    s = np.zeros(sums.shape[1], np.float64)
+    c = np.zeros(sums.shape[1], np.float64)
+    for r in range(sums.shape[0]):
+        s += sums[r]
+        c += counts[r]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(c > 0, (s / np.maximum(c, 1.0)), np.nan).astype(np.float32)
+
+
+def _gather_rows(local: np.ndarray, group=None, device=None) -> np.ndarray:
+    """All-gather one float64 vector of equal length from every rank -> [world, n]."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    dev = torch.device("cpu") if device is None else torch.device(device)
+    buf = torch.from_numpy(np.ascontiguousarray(local, dtype=np.float64)).to(dev)
+    out = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(out, buf, group=group)
+    return np.stack([t.cpu().numpy() for t in out]) if world else np.empty((0, local.size))
+
+
+class DatapointShardedEvaluator:
+    """One rank's view of an evaluation whose datapoints are split over a
+    process group (each rank holds only its columns of X).
+
+    ``evaluator`` is this rank's Evaluator (or any object with ``set_data(X)``,
+    ``eval_sums(pop) -> (sum, count)`` and, for gradients, ``eval_grad(pop)``,
+    ``read_sums()`` and ``read_grad_sums()``)."""
+
+    def __init__(self, evaluator, group=None, device=None, align: int = 1024):
+        import torch.distributed as dist
+
+        if not dist.is_initialized():
+            raise RuntimeError("torch.distributed is not initialised")
+        self.ev = evaluator
+        self.group = group
+        self.device = device
+        self.align = align
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.bounds: Optional[np.ndarray] = None
+
+    def set_data(self, X: Optional[np.ndarray], num_dps: Optional[int] = None, src: int = 0):
+        """Give this rank its shard.  Either every rank passes the whole X
+        (each keeps its columns), or rank `src` passes it and the others pass
+        None: the shards are then scattered from `src` (only a shard crosses
+        to each rank)."""
+        import torch
+        import torch.distributed as dist
+
+        dev = torch.device("cpu") if self.device is None else torch.device(self.device)
+        have = torch.tensor([0 if X is None else 1], dtype=torch.int64, device=dev)
+        dist.all_reduce(have, group=self.group)
+        if int(have.item()) == self.world:
+            X = np.asarray(X, dtype=np.float32)
+            self.bounds = datapoint_bounds(X.shape[1], self.world, self.align)
+            lo, hi = int(self.bounds[self.rank]), int(self.bounds[self.rank + 1])
+            self.ev.set_data(np.ascontiguousarray(X[:, lo:hi]))
+            return
+        shape = torch.zeros(2, dtype=torch.int64, device=dev)
+        if self.rank == src:
+            if X is None:
+                raise ValueError("the scatter source rank must pass the dataset")
+            shape[0], shape[1] = X.shape[0], X.shape[1]
+        dist.broadcast(shape, src=src, group=self.group)
+        rows, cols = int(shape[0].item()), int(shape[1].item())
+        self.bounds = datapoint_bounds(cols, self.world, self.align)
+        width = int(max(int(np.diff(self.bounds).max()), 1))
+        recv = torch.empty((rows, width), dtype=torch.float32, device=dev)
+        chunks = None
+        if self.rank == src:
+            Xa = np.asarray(X, dtype=np.float32)
+            chunks = []
+            for r in range(self.world):
+                c = np.zeros((rows, width), np.float32)
+                lo, hi = int(self.bounds[r]), int(self.bounds[r + 1])
+                c[:, : hi - lo] = Xa[:, lo:hi]
+                chunks.append(torch.from_numpy(c).to(dev))
+        dist.scatter(recv, chunks, src=src, group=self.group)
+        n = int(self.bounds[self.rank + 1] - self.bounds[self.rank])
+        self.ev.set_data(np.ascontiguousarray(recv.cpu().numpy()[:, :n]))
+
+    def eval_mse(self, pop: Population) -> np.ndarray:
+        """MSE of every expression over all shards' datapoints, on every rank."""
+        s, c = self.ev.eval_sums(pop)
+        g = _gather_rows(np.concatenate([np.asarray(s, np.float64), np.asarray(c, np.float64)]),
+                         self.group, self.device)
+        E = pop.num_exprs
+        return combine_sums(g[:, :E], g[:, E:])
+
+    def eval_grad(self, pop: Population):
+        """(MSE [E], d MSE / d constants [C]) over all shards' datapoints."""
+        self.ev.eval_grad(pop)
+        s, c = self.ev.read_sums()
+        gs = self.ev.read_grad_sums()
+        E = pop.num_exprs
+        g = _gather_rows(np.concatenate([np.asarray(s, np.float64), np.asarray(c, np.float64),
+                                         np.asarray(gs, np.float64)]), self.group, self.device)
+        mse = combine_sums(g[:, :E], g[:, E:2 * E])
+        cnt = np.zeros(E, np.float64)
+        gsum = np.zeros(g.shape[1] - 2 * E, np.float64)
+        for r in range(g.shape[0]):
+            cnt += g[r, E:2 * E]
+            gsum += g[r, 2 * E:]
+        per_const = np.repeat(cnt, pop.constant_counts())
+        with np.errstate(invalid="ignore", divide="ignore"):
+            grad = np.where(per_const > 0, gsum / np.maximum(per_const, 1.0), np.nan)
+        return mse, grad.astype(np.float32)
