@@ -184,7 +184,10 @@ int32_t sr_abi_version(void);
 
 /* ---- dataset (reference upload_X branch, cl_gpu_eval.cu:474-489) --------
  * X: host pointer, column-major [(num_vars+1) x num_dps], y in the last row.
- * The data stays on the device until replaced. */
+ * The data stays on the device until replaced.  A new dataset drops the
+ * prepared launch and the subtree cache; a call that fails after its
+ * arguments were accepted (allocation, copy) leaves the context with no
+ * dataset (SR_ERR_NO_DATA until the next successful call). */
 sr_status sr_set_data(sr_context *ctx, const float *X, int32_t num_vars,
                       int64_t num_dps);
 /* Same from the reference's row-pointer form all_vars[0][v][dp] (v <= num_vars). */

@@ -437,6 +437,14 @@ static void reset_prepared(sr_context *ctx) {
   ctx->graph_launches = 0;
 }
 
+// Drop the dataset, the cache built on it and every prepared launch.
+static void invalidate_data(sr_context *ctx) {
+  reset_prepared(ctx);
+  ctx->cache.clear();  // cached subtree values belong to the old data
+  ctx->V = -1;
+  ctx->N = 0;
+}
+
 extern "C" {
 
 int32_t sr_abi_version(void) { return SR_ABI_VERSION; }
@@ -556,6 +564,10 @@ sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, in
                                                " exceeds " + std::to_string(SR_MAX_VARS));
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // Done before X is touched: a failure below (allocation, copy) leaves the
+  // context without data instead of holding launches that point into a
+  // released or half-written X.
+  invalidate_data(ctx);
   const int64_t ldx = std::max<int64_t>(sr::kDataAlign, round_up(num_dps, sr::kDataAlign));
   const size_t rows = static_cast<size_t>(num_vars) + 1;
   SR_TRY_CUDA(ctx, ctx->X.ensure(rows * static_cast<size_t>(ldx)));
@@ -568,8 +580,6 @@ sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, in
   ctx->ldx = ldx;
   ctx->V = num_vars;
   ctx->N = num_dps;
-  ctx->cache.clear();  // cached subtree values belong to the old data
-  reset_prepared(ctx);
   return SR_OK;
 }
 
@@ -583,6 +593,10 @@ static sr_status set_data_host(sr_context *ctx, const float *X, const float *con
                                                " exceeds " + std::to_string(SR_MAX_VARS));
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // Done before X is touched: a failure below (allocation, copy) leaves the
+  // context without data instead of holding launches that point into a
+  // released or half-written X.
+  invalidate_data(ctx);
   const int64_t ldx = std::max<int64_t>(sr::kDataAlign, round_up(num_dps, sr::kDataAlign));
   const size_t rows = static_cast<size_t>(num_vars) + 1;
   SR_TRY_CUDA(ctx, ctx->X.ensure(rows * static_cast<size_t>(ldx)));
@@ -604,8 +618,6 @@ static sr_status set_data_host(sr_context *ctx, const float *X, const float *con
   ctx->ldx = ldx;
   ctx->V = num_vars;
   ctx->N = num_dps;
-  ctx->cache.clear();
-  reset_prepared(ctx);
   return SR_OK;
 }
 

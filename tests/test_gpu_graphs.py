@@ -71,3 +71,32 @@ def test_graph_replay_gradient(mode):
             fin = np.isfinite(g0)
             assert np.array_equal(fin, np.isfinite(g1))
             assert _ulps(g1[fin], g0[fin]).max() <= 2
+
+
+def test_failed_dataset_replacement_drops_the_prepared_graph():
+    """A dataset call that fails after its checks (here: a NULL row in the
+    row-pointer form) leaves the context with no dataset and no prepared
+    launch, never a captured graph pointing into the old X."""
+    import ctypes
+    w = synth.batched_workload(seed=12, E=200, N=30_000)
+    with sg.Evaluator(device=0, use_graphs=True) as ev:
+        ev.set_data(w.X)
+        ev.prepare(w.population)
+        ev.launch()
+        want = ev.read_mse()
+        V, N = w.num_vars, w.num_dps
+        rows = (ctypes.POINTER(ctypes.c_float) * (V + 1))()
+        keep = [np.ascontiguousarray(w.X[v]) for v in range(V + 1)]
+        for v in range(V):
+            rows[v] = keep[v].ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        rows[V] = ctypes.POINTER(ctypes.c_float)()  # NULL y row
+        st = _lib.lib.sr_set_data_rows(ev._ctx, rows, V, N)
+        assert st == _lib.SR_ERR_INVALID_ARGUMENT
+        assert _lib.lib.sr_launch(ev._ctx) == _lib.SR_ERR_INVALID_ARGUMENT  # nothing prepared
+        with pytest.raises(sg.SrError) as ei:
+            ev.eval_mse(w.population)
+        assert ei.value.status == _lib.SR_ERR_NO_DATA
+        ev.set_data(w.X)
+        ev.prepare(w.population)
+        ev.launch()
+        assert _same(ev.read_mse(), want)
