@@ -181,6 +181,13 @@ const char *sr_status_string(sr_status s);
 /* Message of the last failed call on ctx ("" if none). */
 const char *sr_last_error(const sr_context *ctx);
 int32_t sr_abi_version(void);
+/* Fault injection for tests (process-wide): with n > 0 the n-th following
+ * device or pinned-host allocation made by the library fails as if the
+ * memory were exhausted (the call returns SR_ERR_OUT_OF_MEMORY and the
+ * context stays usable); n = 0 disables it.  The reference has no
+ * counterpart (its CUDA_CHECK exits the process on any failure,
+ * cl_gpu_common.h:15-23). */
+sr_status sr_inject_allocation_failure(int64_t n);
 
 /* ---- dataset (reference upload_X branch, cl_gpu_eval.cu:474-489) --------
  * X: host pointer, column-major [(num_vars+1) x num_dps], y in the last row.

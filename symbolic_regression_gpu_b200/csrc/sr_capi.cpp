@@ -24,6 +24,7 @@
 #include "sr_detect_gpu.hpp"
 #include "sr_evolve.hpp"
 #include "sr_kernels.hpp"
+#include "sr_trace.hpp"
 
 using sr::Instr;
 using sr::ProgramSet;
@@ -110,6 +111,7 @@ sr_status check_population(sr_context *ctx, const sr_population *pop) {
 // Compile expressions [0, E) of a CSR population into ps (pinned staging).
 sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *val,
                       const int64_t *off, const int32_t *hints, ProgramSet &ps) {
+  SR_TRACE("sr: compile");
   ps.E = E;
   ps.cost.assign(static_cast<size_t>(E), 0.f);
   ps.n_const.assign(static_cast<size_t>(E), 0);
@@ -244,6 +246,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
 }
 
 sr_status upload_groups(sr_context *ctx, ProgramSet &ps) {
+  SR_TRACE("sr: upload groups");
   const size_t ng = static_cast<size_t>(std::max(ps.plan.n_groups * ps.plan.G, 1));
   ctx->prep_stats.h2d_bytes += static_cast<int64_t>(ng * sizeof(int32_t));
   SR_TRY_CUDA(ctx, ps.group.ensure(ng));
@@ -253,6 +256,7 @@ sr_status upload_groups(sr_context *ctx, ProgramSet &ps) {
 }
 
 sr_status upload_code(sr_context *ctx, ProgramSet &ps) {
+  SR_TRACE("sr: upload code");
   const int E = ps.E;
   SR_TRY_CUDA(ctx, ps.code.ensure(static_cast<size_t>(ps.n_instr + 1)));
   SR_TRY_CUDA(ctx, ps.off.ensure(static_cast<size_t>(std::max(E, 1))));
@@ -362,6 +366,7 @@ void save_tune_cache(const sr_context *ctx) {
 
 // Times each candidate shape on the prepared population and keeps the fastest.
 sr_status autotune_main(sr_context *ctx, const std::string &key) {
+  SR_TRACE("sr: autotune");
   static const int kCand[][2] = {{16, 8}, {16, 16}, {8, 8}, {8, 16}, {4, 8}, {4, 16}};
   float best = 1e30f;
   int best_dpt = 8, best_w = 8;
@@ -430,6 +435,7 @@ static cudaError_t record_event(sr_context *ctx, int k) {
 // point into buffers that the next prepare / set_data may move).
 static void reset_prepared(sr_context *ctx) {
   ctx->mode = sr::Mode::kNone;
+  ctx->cache.rollback();  // subtrees of a launch that never ran hold no values
   if (ctx->graph_exec) {
     cudaGraphExecDestroy(ctx->graph_exec);
     ctx->graph_exec = nullptr;
@@ -448,6 +454,12 @@ static void invalidate_data(sr_context *ctx) {
 extern "C" {
 
 int32_t sr_abi_version(void) { return SR_ABI_VERSION; }
+
+sr_status sr_inject_allocation_failure(int64_t n) {
+  if (n < 0) return SR_ERR_INVALID_ARGUMENT;
+  sr::alloc_fault_countdown().store(n);
+  return SR_OK;
+}
 
 const char *sr_status_string(sr_status s) {
   switch (s) {
@@ -556,6 +568,7 @@ sr_status sr_destroy(sr_context *ctx) {
 
 sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, int32_t num_vars,
                              int64_t num_dps) {
+  SR_TRACE("sr_set_data_device");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (num_vars < 0 || num_dps < 0 || (num_dps > 0 && !X_dev) || ld < num_dps)
     return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad dataset arguments");
@@ -585,6 +598,7 @@ sr_status sr_set_data_device(sr_context *ctx, const float *X_dev, int64_t ld, in
 
 static sr_status set_data_host(sr_context *ctx, const float *X, const float *const *rows_ptr,
                                int32_t num_vars, int64_t num_dps) {
+  SR_TRACE("sr_set_data");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (num_vars < 0 || num_dps < 0 || (num_dps > 0 && !X && !rows_ptr))
     return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad dataset arguments");
@@ -634,6 +648,7 @@ sr_status sr_set_data_rows(sr_context *ctx, const float *const *rows, int32_t nu
 // ---- prepare --------------------------------------------------------------
 
 static sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
+  SR_TRACE("sr: prepare plain");
   sr::PlainSet &ps = ctx->plain;
   const int E = pop->num_exprs;
   const int64_t T = pop->offsets[E];
@@ -708,6 +723,7 @@ static sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
 static sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, const double *val,
                                   const int64_t *off, int min_size, int min_freq,
                                   sr::Detection &out) {
+  SR_TRACE("sr: detect (device)");
   out = sr::Detection{};
   out.total_tokens = E > 0 ? off[E] - off[0] : 0;
   const int64_t T = out.total_tokens;
@@ -814,6 +830,7 @@ static sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, co
 }
 
 static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint32_t flags) {
+  SR_TRACE("sr: prepare cached");
   const int E = pop->num_exprs;
   const int64_t T = pop->offsets[E];
   // Validate first so that malformed input never reaches the cache.
@@ -834,20 +851,24 @@ static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint3
   const int threads = host_threads(ctx);
   const double t0 = now_ms();
   sr::Detection det;
-  if (ctx->opts.device_detect)
+  if (ctx->opts.device_detect) {
     SR_TRY(detect_on_device(ctx, E, pop->tokens, pop->values, pop->offsets,
                             ctx->opts.min_subtree_size, ctx->opts.min_subtree_freq, det));
-  else
+  } else {
+    SR_TRACE("sr: detect (host)");
     sr::detect_common_subtrees(E, pop->tokens, pop->values, pop->offsets,
                                ctx->opts.min_subtree_size, ctx->opts.min_subtree_freq, threads,
                                det);
+  }
   ctx->prep_stats.detect_time_ms = now_ms() - t0;
   ctx->prep_stats.num_subtrees = static_cast<int32_t>(det.groups.size());
   ctx->prep_stats.avg_subtree_size = det.avg_subtree_size;
   ctx->prep_stats.coverage = det.coverage;
 
   // Cache update (reference cl_gpu_eval.cu:384-396): new keys get the next
-  // free slot until the capacity is reached.
+  // free slot until the capacity is reached.  They stay pending until this
+  // prepare's launch is enqueued (sr_launch commits them).
+  ctx->cache.begin_pending();
   std::vector<int32_t> sub_tok;
   std::vector<double> sub_val;
   std::vector<int64_t> sub_off{0};
@@ -860,6 +881,7 @@ static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint3
     if (ctx->cache.used >= ctx->cache.capacity) continue;
     const int32_t slot = ctx->cache.used++;
     ctx->cache.slot_of.emplace(key, slot);
+    ctx->cache.pending.push_back(key);
     sub_tok.insert(sub_tok.end(), t, t + g.size);
     sub_val.insert(sub_val.end(), v, v + g.size);
     sub_off.push_back(static_cast<int64_t>(sub_tok.size()));
@@ -914,6 +936,7 @@ sr_status launch_grad(sr_context *ctx);
 extern "C" {
 
 sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) {
+  SR_TRACE("sr_prepare");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   SR_TRY(check_population(ctx, pop));
@@ -991,6 +1014,7 @@ static sr_status enqueue_launch(sr_context *ctx, int *launches_out) {
 }
 
 sr_status sr_launch(sr_context *ctx) {
+  SR_TRACE("sr_launch");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (ctx->E == 0) return SR_OK;
   if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing prepared");
@@ -1022,6 +1046,7 @@ sr_status sr_launch(sr_context *ctx) {
   } else {
     SR_TRY(enqueue_launch(ctx, &launches));
   }
+  ctx->cache.commit();  // the subtree launch that writes the new cached values is enqueued
   ctx->timing_valid = true;
   ctx->prep_stats.kernel_launches = launches;
   return SR_OK;
@@ -1033,6 +1058,7 @@ static sr_status check_device_error(sr_context *ctx) {
   *ctx->h_error = 0;
   cudaMemsetAsync(ctx->d_error, 0, sizeof(int32_t), ctx->stream);
   cudaStreamSynchronize(ctx->stream);
+  ctx->cache.clear();  // the failed launch may have left cached values unwritten
   if (code & sr::kDevErrTimeout)
     return ctx->fail(SR_ERR_DEVICE_TIMEOUT, "a device-side wait exceeded its time limit");
   return ctx->fail(SR_ERR_DEVICE_CHECK, "device bounds check failed");
@@ -1060,8 +1086,10 @@ static void fill_stats(sr_context *ctx, sr_stats *st) {
 }
 
 sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats) {
+  SR_TRACE("sr_read_mse");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (ctx->E == 0) return SR_OK;
+  if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing launched");
   if (!mse_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "mse_out is NULL");
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_mse.p, ctx->mse.p, ctx->E * sizeof(float),
@@ -1076,6 +1104,7 @@ sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats) {
 }
 
 sr_status sr_read_sums(sr_context *ctx, double *sum_out, double *count_out) {
+  SR_TRACE("sr_read_sums");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (ctx->E == 0) return SR_OK;
   if (ctx->mode == sr::Mode::kNone) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "nothing launched");
@@ -1161,6 +1190,7 @@ sr_status sr_device_mse(sr_context *ctx, float **mse_dev) {
 
 sr_status sr_eval_mse(sr_context *ctx, const sr_population *pop, uint32_t flags, float *mse_out,
                       sr_stats *stats) {
+  SR_TRACE("sr_eval_mse");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   const double t0 = now_ms();
   SR_TRY(sr_prepare(ctx, pop, flags));
@@ -1176,6 +1206,7 @@ sr_status sr_eval_mse(sr_context *ctx, const sr_population *pop, uint32_t flags,
 
 sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop, int64_t dp_begin,
                               int64_t dp_count, float *pred_out) {
+  SR_TRACE("sr_eval_predictions");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   SR_TRY(check_population(ctx, pop));
@@ -1495,6 +1526,7 @@ extern "C" {
 
 sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode, float *mse_out,
                        float *grad_out, sr_stats *stats) {
+  SR_TRACE("sr_eval_grad");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   if (mode != SR_GRAD_CHECKPOINT && mode != SR_GRAD_RECOMPUTE)
@@ -1519,6 +1551,7 @@ sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode, 
 sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
                                 const sr_adam_options *adam, float *const_out, float *mse_out,
                                 sr_stats *stats) {
+  SR_TRACE("sr_optimize_constants");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   if (!adam || adam->steps < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad Adam options");
@@ -1575,6 +1608,7 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
 }
 
 sr_status sr_eval_mse_fp64(sr_context *ctx, const sr_population *pop, double *mse64_out) {
+  SR_TRACE("sr_eval_mse_fp64");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   SR_TRY(check_population(ctx, pop));
@@ -1694,6 +1728,7 @@ extern "C" {
 
 sr_status sr_evolve_init(sr_context *ctx, const sr_evolve_options *opts, int32_t num_exprs,
                          int32_t stride, int32_t *tokens, float *values, int32_t *lengths) {
+  SR_TRACE("sr_evolve_init");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   sr::EvolveParams p;
@@ -1710,6 +1745,7 @@ sr_status sr_evolve_step(sr_context *ctx, const sr_evolve_options *opts, int32_t
                          int32_t num_exprs, int32_t stride, const float *fitness,
                          const int32_t *tokens, const float *values, const int32_t *lengths,
                          int32_t *tokens_out, float *values_out, int32_t *lengths_out) {
+  SR_TRACE("sr_evolve_step");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   sr::EvolveParams p;
@@ -1752,6 +1788,7 @@ sr_status sr_evolve_step(sr_context *ctx, const sr_evolve_options *opts, int32_t
 sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
                                        const float *values, const int32_t *lengths,
                                        int32_t num_exprs, int32_t stride) {
+  SR_TRACE("sr_prepare_device_population");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   if (num_exprs < 0 || stride < 1 || stride > SR_EVOLVE_MAX_STRIDE)
@@ -1876,6 +1913,7 @@ sr_status sr_detect_subtrees(const sr_population *pop, int32_t min_size, int32_t
                              int32_t max_groups, sr_detect_result *res, int32_t *group_expr,
                              int32_t *group_pos, int32_t *group_size, int32_t *group_count,
                              uint64_t *group_key) {
+  SR_TRACE("sr_detect_subtrees");
   if (!pop || !res || pop->num_exprs < 0 || min_size < 1 || min_freq < 1)
     return SR_ERR_INVALID_ARGUMENT;
   if (pop->num_exprs > 0 && (!pop->tokens || !pop->values || !pop->offsets))
@@ -1906,6 +1944,7 @@ sr_status sr_detect_subtrees_device(sr_context *ctx, const sr_population *pop, i
                                     int32_t min_freq, int32_t max_groups, sr_detect_result *res,
                                     int32_t *group_expr, int32_t *group_pos, int32_t *group_size,
                                     int32_t *group_count, uint64_t *group_key) {
+  SR_TRACE("sr_detect_subtrees_device");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   if (!pop || !res || pop->num_exprs < 0 || min_size < 1 || min_freq < 1)

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <string>
@@ -17,7 +18,23 @@
 
 namespace sr {
 
+// Host-side fault injection for tests (sr_inject_allocation_failure): when the
+// countdown is n > 0, the n-th following DevBuf / PinnedBuf allocation fails
+// with cudaErrorMemoryAllocation without reaching the allocator (once).
+inline std::atomic<int64_t> &alloc_fault_countdown() {
+  static std::atomic<int64_t> countdown{0};
+  return countdown;
+}
+inline bool alloc_fault_fires() {
+  std::atomic<int64_t> &c = alloc_fault_countdown();
+  int64_t v = c.load(std::memory_order_relaxed);
+  while (v > 0)
+    if (c.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return v == 1;
+  return false;
+}
+
 // Grow-only device buffer.  Callers synchronise the stream before growing.
+// A failed growth leaves the buffer empty (p == nullptr, cap == 0).
 template <class T>
 struct DevBuf {
   T *p = nullptr;
@@ -35,6 +52,7 @@ struct DevBuf {
     if (p && n <= cap) return cudaSuccess;
     const size_t want = std::max<size_t>(n + n / 4, 64);
     release();
+    if (alloc_fault_fires()) return cudaErrorMemoryAllocation;
     const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
@@ -63,6 +81,7 @@ struct PinnedBuf {
     if (p && n <= cap) return cudaSuccess;
     const size_t want = std::max<size_t>(n + n / 4, 64);
     release();
+    if (alloc_fault_fires()) return cudaErrorMemoryAllocation;
     const cudaError_t e = cudaMallocHost(&p, want * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;

@@ -57,9 +57,27 @@ struct SubtreeCache {
   std::unordered_map<uint64_t, int32_t> slot_of;
   int32_t used = 0;
   int32_t capacity = 2048;
+  // Keys inserted by a prepare whose launch has not been enqueued yet: their
+  // values exist only once that launch runs, so they are taken out again if
+  // the prepared launch is dropped (or its prepare fails) before that.
+  std::vector<uint64_t> pending;
+  int32_t pending_base = 0;
   void clear() {
     slot_of.clear();
     used = 0;
+    pending.clear();
+    pending_base = 0;
+  }
+  void begin_pending() {
+    pending.clear();
+    pending_base = used;
+  }
+  void commit() { pending.clear(); }
+  void rollback() {
+    if (pending.empty()) return;
+    for (uint64_t k : pending) slot_of.erase(k);
+    used = pending_base;
+    pending.clear();
   }
 };
 

@@ -84,3 +84,19 @@ def test_cache_invalidated_by_new_data(work):
         cached = ev.eval_mse(work.population, cache=True)
         plain = ev.eval_mse(work.population)
     assert _bits_equal(cached, plain)
+
+
+def test_prepare_without_launch_leaves_no_phantom_cache_entries(work):
+    """A cached prepare inserts the new subtrees' keys, whose values exist only
+    once its launch runs.  A second prepare before any launch must not find
+    those keys (it would read cache rows nothing has written)."""
+    with sg.Evaluator(device=0) as ev:
+        ev.set_data(work.X)
+        want = ev.eval_mse(work.population, cache=True, clear_cache=True)
+        ev.prepare(work.population, cache=True, clear_cache=True)  # never launched
+        ev.prepare(work.population, cache=True)
+        ev.launch()
+        got = ev.read_mse()
+        st = ev.stats
+    assert st.new_subtrees > 0  # the dropped prepare's subtrees are evaluated again
+    assert _bits_equal(got, want)
