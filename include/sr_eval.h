@@ -470,10 +470,19 @@ sr_status sr_load_population(const char *path, int32_t *num_exprs, int64_t *num_
 
 sr_status sr_get_stream(sr_context *ctx, void **stream);
 sr_status sr_synchronize(sr_context *ctx);
-/* Measured per-SM pipe peaks on this device (FP32 FMA lanes/clock and MUFU
- * ex2 lanes/clock) from two short microbenchmarks, plus the SM count. */
+/* Measured device-wide pipe peaks (FP32 FMA and MUFU rsqrt thread-operations
+ * per second) from two short microbenchmarks, plus the SM count. */
 sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s,
                            double *sfu_ops_per_s, int32_t *num_sms);
+/* Measured throughput (evaluations per second, whole device) of each listed
+ * operator's FP32 semantics alone: 8 independent evaluations per thread per
+ * iteration, each added into an accumulator, operands in [-3, 3] (second
+ * operand in [0.5, 3]).  Operator 0 times the harness alone (one add per
+ * evaluation).  The accurate-operator bound of a population is the sum over
+ * its operator tokens of 1 / rate (less the harness), times the datapoints.
+ * Operators: 0-27 and 32.  No reference counterpart. */
+sr_status sr_measure_operator_rates(sr_context *ctx, const int32_t *ops, int32_t n_ops,
+                                   double *evals_per_s);
 
 #ifdef __cplusplus
 }

@@ -1892,6 +1892,38 @@ sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s, double *sfu_
   return SR_OK;
 }
 
+sr_status sr_measure_operator_rates(sr_context *ctx, const int32_t *ops, int32_t n_ops,
+                                   double *evals_per_s) {
+  SR_TRACE("sr_measure_operator_rates");
+  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
+  if (n_ops < 0 || (n_ops > 0 && (!ops || !evals_per_s)))
+    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad operator list");
+  for (int32_t i = 0; i < n_ops; ++i)
+    if (!(ops[i] >= 0 && ops[i] <= 27) && ops[i] != static_cast<int32_t>(sr::kOpExpClamp))
+      return ctx->fail(SR_ERR_BAD_TOKEN, "operator " + std::to_string(ops[i]) + " has no rate kernel");
+  DeviceScope scope(ctx->device);
+  float *dummy = nullptr;
+  SR_TRY_CUDA(ctx, cudaMalloc(&dummy, 1024 * sizeof(float)));
+  const int blocks = ctx->num_sms * 8, threads = 256, iters = 256;
+  for (int32_t i = 0; i < n_ops; ++i) {
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(ctx->ev[4], ctx->stream);
+      const cudaError_t e = sr::launch_op_rate(ops[i], dummy, blocks, threads, iters, ctx->stream);
+      cudaEventRecord(ctx->ev[5], ctx->stream);
+      if (e != cudaSuccess || cudaEventSynchronize(ctx->ev[5]) != cudaSuccess) {
+        cudaFree(dummy);
+        return cuda_fail(ctx, e != cudaSuccess ? e : cudaGetLastError(), "operator rate");
+      }
+      const float ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+      if (rep > 0) best = std::min(best, ms);
+    }
+    evals_per_s[i] = static_cast<double>(blocks) * threads * iters * 8.0 / (best * 1e-3);
+  }
+  cudaFree(dummy);
+  return SR_OK;
+}
+
 }  // extern "C"
 
 // ---- host-only helpers ------------------------------------------------------

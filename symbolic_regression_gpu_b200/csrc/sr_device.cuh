@@ -474,6 +474,43 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
   }                                                                            \
     SR_CALL1(v_exp)
 
+// Inline forms of exp (a few instructions around ex2), sqrt and the IEEE
+// division: the same functions expanded at their case instead of called two
+// datapoints at a time, for the switches of the protected profile and of its
+// out-of-line path, in launches of at most 8 datapoints per thread.  There a
+// call cost more than these bodies (batched population forward 78.7 -> 73.7
+// ms, subtree-cache population 44.9 -> 42.0 ms, results bit-identical); at 16
+// datapoints per thread the copies cost more than the calls (36.8 -> 40.6 ms).
+// sin / cos / log stay out of line (inlined, the instruction cache overflows:
+// 100.6 ms with sin and cos inline), and so do all of them in the
+// every-operator switch (kOpsAll), which inlining made slower (150.1 -> 162.3
+// ms on a population that uses every operator).
+constexpr int kInlineMaxDpt = 8;  // wider launches call them (16 copies overflow the I-cache)
+#define SR_C_INL_OR(CASE, INLINE_STMT, CALLED)                                 \
+  case CASE:                                                                   \
+    if constexpr (DPT <= kInlineMaxDpt) {                                      \
+      _Pragma("unroll") for (int k = 0; k < DPT; ++k) { INLINE_STMT; }         \
+    } else {                                                                   \
+      CALLED                                                                   \
+    }                                                                          \
+    break;
+#define SR_C_EXPC_INL                                                          \
+  SR_C_INL_OR(32, T[k] = expf(fminf(T[k], 80.0f)),                             \
+              _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = fminf(T[k], 80.0f); \
+              SR_MAP1(v_exp, T, T))
+#define SR_C_LSQRT_INL                                                         \
+  SR_C_INL_OR(27, T[k] = __fsqrt_rn(fabsf(T[k])),                              \
+              _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = fabsf(T[k]); \
+              SR_MAP1(v_sqrt, T, T))
+#define SR_C_LDIV_INL                                                          \
+  SR_C_INL_OR(8, T[k] = __fdiv_rn(T[k], loose_denom(b[k])),                    \
+              _Pragma("unroll") for (int k = 0; k < DPT; ++k) b[k] = loose_denom(b[k]); \
+              SR_MAP2(v_div, T, T, b))
+#define SR_C_RLDIV_INL                                                         \
+  SR_C_INL_OR(48, T[k] = __fdiv_rn(b[k], loose_denom(T[k])),                   \
+              _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = loose_denom(T[k]); \
+              SR_MAP2(v_div, T, b, T))
+
 // Operator profiles (kOpsAll / kOpsProtected and the host-side membership
 // test live in sr_internal.hpp).  kOpsAll dispatches every operator inline;
 // kOpsProtected dispatches + - *, protected division, sin, cos, exp clamped
@@ -501,6 +538,21 @@ __device__ __forceinline__ void apply_op_any(uint32_t op, float (&T)[DPT], float
 // Out-of-line entry of the operators outside a profile; T and b travel
 // through the caller's stack (copies, so the caller's arrays stay in
 // registers).
+// The complete switch of the out-of-line path (apply_op_cold), with the
+// inline forms above.
+template <int DPT>
+__device__ __forceinline__ void apply_op_cold_switch(uint32_t op, float (&T)[DPT],
+                                                     float (&b)[DPT]) {
+  switch (op) {
+    SR_C_NONE SR_C_ADD SR_C_SUB SR_C_RSUB SR_C_MUL SR_C_DIV SR_C_RDIV SR_C_POW SR_C_RPOW
+    SR_C_MIN SR_C_RMIN SR_C_MAX SR_C_RMAX SR_C_LDIV_INL SR_C_RLDIV_INL SR_C_LPOW SR_C_RLPOW
+    SR_C_SIN SR_C_COS SR_C_TAN SR_C_SINH SR_C_COSH SR_C_TANH SR_C_EXP SR_C_LOG SR_C_INV
+    SR_C_ASIN SR_C_ACOS SR_C_ATAN SR_C_LLOG SR_C_LINV SR_C_ABS SR_C_NEG SR_C_SQRT SR_C_LSQRT_INL
+    SR_C_EXPC_INL
+    default: SR_EACH(T[k] = 0.0f)
+  }
+}
+
 template <int DPT>
 __device__ __noinline__ void apply_op_cold(uint32_t op, float *T, float *b) {
   float t[DPT], bb[DPT];
@@ -509,7 +561,7 @@ __device__ __noinline__ void apply_op_cold(uint32_t op, float *T, float *b) {
     t[k] = T[k];
     bb[k] = b[k];
   }
-  apply_op_any<DPT>(op, t, bb);
+  apply_op_cold_switch<DPT>(op, t, bb);
 #pragma unroll
   for (int k = 0; k < DPT; ++k) T[k] = t[k];
 }
@@ -529,8 +581,8 @@ template <int DPT, int OPS>
 __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b)[DPT]) {
   if constexpr (OPS == kOpsProtected) {
     switch (op) {
-      SR_C_NONE SR_C_ADD SR_C_SUB SR_C_RSUB SR_C_MUL SR_C_LDIV SR_C_RLDIV SR_C_SIN SR_C_COS
-      SR_C_EXPC SR_C_LLOG SR_C_LSQRT
+      SR_C_NONE SR_C_ADD SR_C_SUB SR_C_RSUB SR_C_MUL SR_C_LDIV_INL SR_C_RLDIV_INL SR_C_SIN
+      SR_C_COS SR_C_EXPC_INL SR_C_LLOG SR_C_LSQRT_INL
       SR_C_COLD
     }
   } else {

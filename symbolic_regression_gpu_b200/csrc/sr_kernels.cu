@@ -28,6 +28,8 @@
 //                             (4 expressions x 128 datapoints per block, token
 //                             stack in local memory), fused MSE reduction.
 //  pipe microbenchmarks       FP32 FMA and MUFU throughput of the device.
+//  op_rate_kernel             throughput of each operator's FP32 semantics alone
+//                             (the accurate-operator bound of the interpreter).
 //
 // Reference counterparts: eval_subtrees_kernel / eval_skeletons_kernel /
 // reduce_mse_kernel (src/cleaned/cl_gpu_eval.cu:60-245) and eval_simple_kernel
@@ -391,6 +393,50 @@ __global__ void mufu_pipe_kernel(float *out, int iters) {
   if (s == 1234.5f) out[threadIdx.x] = s;
 }
 
+// Throughput of one operator's FP32 semantics with nothing around it: every
+// thread evaluates OP on 8 independent operand pairs per iteration (operands
+// made opaque to the compiler each time, so nothing is hoisted) and adds the
+// results.  With OP = 0 (the identity) it times the harness alone.
+template <int OP>
+__global__ void op_rate_kernel(float *out, int iters) {
+  float x[8], y[8], acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) * 8u + static_cast<uint32_t>(k);
+    h ^= h >> 16;
+    h *= 0x7feb352dU;
+    h ^= h >> 15;
+    h *= 0x846ca68bU;
+    h ^= h >> 16;
+    x[k] = -3.0f + 6.0f * static_cast<float>(h & 0xFFFFFFu) * (1.0f / 16777216.0f);
+    y[k] = 0.5f + 2.5f * static_cast<float>(h >> 8) * (1.0f / 16777216.0f);
+    acc[k] = 0.0f;
+  }
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      float a = x[k], b = y[k];
+      asm volatile("" : "+f"(a), "+f"(b));
+      acc[k] = __fadd_rn(acc[k], op_apply(OP, a, b));
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += acc[k];
+  if (s == 1234.5f) out[threadIdx.x] = s;  // keeps the loop alive
+}
+
+template <int... OPS>
+struct OpRateTable {
+  static const void *get(int op) {
+    const void *fn = nullptr;
+    ((fn = (op == OPS) ? reinterpret_cast<const void *>(&op_rate_kernel<OPS>) : fn), ...);
+    return fn;
+  }
+};
+using OpRates = OpRateTable<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18,
+                            19, 20, 21, 22, 23, 24, 25, 26, 27, 32>;
+
 }  // namespace
 
 size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span) {
@@ -498,6 +544,14 @@ cudaError_t launch_sums(const double2 *partial, int n_spans, int E, double2 *sum
   if (E <= 0) return cudaSuccess;
   sums_kernel<<<(E + 255) / 256, 256, 0, stream>>>(partial, n_spans, E, sums);
   return cudaGetLastError();
+}
+
+cudaError_t launch_op_rate(int op, float *out, int blocks, int threads, int iters,
+                           cudaStream_t stream) {
+  const void *fn = OpRates::get(op);
+  if (!fn) return cudaErrorInvalidValue;
+  void *params[] = {&out, &iters};
+  return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), params, 0, stream);
 }
 
 cudaError_t launch_pipe_bench(bool mufu, float *out, int blocks, int threads,

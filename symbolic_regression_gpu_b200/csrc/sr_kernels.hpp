@@ -41,6 +41,10 @@ cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *of
 cudaError_t launch_fp64(const int32_t *tok, const float *val, const int64_t *off,
                        const int32_t *len, const float *X, int64_t ldx, int V, int64_t N, int E,
                        double2 *partial, int n_dpblocks, double *mse64, cudaStream_t stream);
+// Operator-throughput microbenchmark (op_rate_kernel<op>); op 0 times the
+// harness alone.  cudaErrorInvalidValue for an opcode without an instance.
+cudaError_t launch_op_rate(int op, float *out, int blocks, int threads, int iters,
+                           cudaStream_t stream);
 cudaError_t launch_pipe_bench(bool mufu, float *out, int blocks, int threads,
                               int iters, cudaStream_t stream);
 

@@ -271,6 +271,30 @@ class Evaluator:
                                               ctypes.byref(n)), "sr_measure_pipes")
         return f.value, s.value, n.value
 
+    def measure_operator_rates(self, ops) -> dict:
+        """{operator: evaluations/s} of each operator's FP32 semantics alone on
+        this device (operator 0 = the measuring harness alone)."""
+        arr = np.ascontiguousarray(list(ops), dtype=np.int32)
+        out = np.zeros(max(arr.size, 1), np.float64)
+        self._check(_lib.lib.sr_measure_operator_rates(
+            self._ctx, arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(arr.size),
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "sr_measure_operator_rates")
+        return {int(o): float(r) for o, r in zip(arr, out)}
+
+
+def operator_bound_seconds(pop: Population, num_dps: int, rates: dict,
+                           fp32_ops_per_s: float) -> float:
+    """Accurate-operator bound of one evaluation of `pop`: every operator token
+    at every datapoint costs 1 / rate of its operator less the harness's own
+    cost (rates[0]), at least one FP32 instruction; leaves cost nothing."""
+    toks = pop.tokens[pop.tokens > 0]
+    ops, counts = np.unique(toks, return_counts=True)
+    base = 1.0 / rates[0]
+    per_dp = 0.0
+    for o, c in zip(ops, counts):
+        per_dp += c * max(1.0 / rates[int(o)] - base, 1.0 / fp32_ops_per_s)
+    return per_dp * num_dps
+
 
 # ---- host-only helpers (no GPU needed) ------------------------------------
 
