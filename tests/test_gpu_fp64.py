@@ -3,7 +3,7 @@ FP32 result) against the CPU FP64 oracle (oracle/sr_oracle.c, the same
 semantics in double): CUDA's and glibc's double-precision functions are both
 within a few ulp, so the MSEs agree to ~1e-12 relative (1e-9 allowed where
 pred - y cancels); NaN exactly where the oracle has no valid datapoint.
-The FP32 evaluator's error against it is the north-star bar: <= 1e-5
+The FP32 evaluator's error against it is the accuracy target: <= 1e-5
 relative for the MSE of smooth populations."""
 import numpy as np
 import pytest
