@@ -220,8 +220,19 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
     return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape needs " + std::to_string(p.smem) +
                                              " bytes of shared memory");
   p.n_spans = (ctx->N == 0 || E == 0) ? 0 : static_cast<int>((ctx->N + span - 1) / span);
-  if (!pred && static_cast<double>(p.n_spans) * E * 16.0 > 8.0 * (1ull << 30))
-    return ctx->fail(SR_ERR_UNSUPPORTED, "partial-sum buffer would exceed 8 GiB");
+  // One FP64 (sum, count) per (span, expression): 16 B x E x N / span.  It is
+  // sized against the device's memory (the allocation itself reports
+  // SR_ERR_OUT_OF_MEMORY when the free memory is short).
+  if (!pred) {
+    size_t free_b = 0, total_b = 0;
+    SR_TRY_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b));
+    const double need = static_cast<double>(p.n_spans) * E * 16.0;
+    if (need > 0.9 * static_cast<double>(total_b))
+      return ctx->fail(SR_ERR_UNSUPPORTED,
+                       "partial-sum buffer (" + std::to_string(static_cast<int64_t>(need)) +
+                           " bytes) exceeds the device memory; split the population or the "
+                           "datapoints");
+  }
   int bps = 0;
   SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache, p.smem, W, &bps));
   if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
