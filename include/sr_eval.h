@@ -476,9 +476,9 @@ sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s,
                            double *sfu_ops_per_s, int32_t *num_sms);
 /* Measured throughput (evaluations per second, whole device) of each listed
  * operator's FP32 semantics alone: 8 independent evaluations per thread per
- * iteration, each added into an accumulator, operands in [-3, 3] (second
- * operand in [0.5, 3]).  Operator 0 times the harness alone (one add per
- * evaluation).  The accurate-operator bound of a population is the sum over
+ * iteration, each added into an accumulator, first operand in [-3, 3] moving
+ * by 1e-6 per iteration, second operand in [0.5, 3].  Operator 0 times the
+ * harness alone (two adds per evaluation).  The accurate-operator bound of a population is the sum over
  * its operator tokens of 1 / rate (less the harness), times the datapoints.
  * Operators: 0-27 and 32.  No reference counterpart. */
 sr_status sr_measure_operator_rates(sr_context *ctx, const int32_t *ops, int32_t n_ops,

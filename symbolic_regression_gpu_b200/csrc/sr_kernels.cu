@@ -394,9 +394,11 @@ __global__ void mufu_pipe_kernel(float *out, int iters) {
 }
 
 // Throughput of one operator's FP32 semantics with nothing around it: every
-// thread evaluates OP on 8 independent operand pairs per iteration (operands
-// made opaque to the compiler each time, so nothing is hoisted) and adds the
-// results.  With OP = 0 (the identity) it times the harness alone.
+// thread evaluates OP on 8 independent operand pairs per iteration and adds
+// the results.  The first operand moves by a tiny step every iteration, so no
+// evaluation is loop-invariant (an empty inline-asm barrier was not enough:
+// the code generator still hoisted some functions out of the loop).  With
+// OP = 0 (the identity) it times the harness alone (two adds per evaluation).
 template <int OP>
 __global__ void op_rate_kernel(float *out, int iters) {
   float x[8], y[8], acc[8];
@@ -413,11 +415,11 @@ __global__ void op_rate_kernel(float *out, int iters) {
     acc[k] = 0.0f;
   }
   for (int i = 0; i < iters; ++i) {
+    const float step = static_cast<float>(i) * 1e-6f;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      float a = x[k], b = y[k];
-      asm volatile("" : "+f"(a), "+f"(b));
-      acc[k] = __fadd_rn(acc[k], op_apply(OP, a, b));
+      const float a = __fadd_rn(x[k], step);
+      acc[k] = __fadd_rn(acc[k], op_apply(OP, a, y[k]));
     }
   }
   float s = 0.f;
