@@ -187,16 +187,20 @@ sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *
   return SR_OK;
 }
 
+// Operator profile of a compiled set (the evaluation launches; prediction
+// launches always use kOpsAll).
+bool protected_profile(const ProgramSet &ps) {
+  return ps.n_instr > 0 &&
+         static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr;
+}
+
 // Launch shape: groups of G cost-sorted expressions x spans of datapoints.
 sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
                    int span_target = 1024, int per_warp = 4) {
   sr::Plan p;
   p.dpt = dpt;
   p.W = W;
-  p.ops = (!pred && ps.n_instr > 0 &&
-           static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr)
-              ? sr::kOpsProtected
-              : sr::kOpsAll;
+  p.ops = (!pred && protected_profile(ps)) ? sr::kOpsProtected : sr::kOpsAll;
   p.cache = !pred && ps.cache_refs;
   p.smax = std::max(ps.smax, 0);
   p.s_smem = std::min(p.smax, sr::smem_spill_slots(dpt));
@@ -333,8 +337,7 @@ std::string tune_key(const sr_context *ctx, const ProgramSet &ps) {
   const int lg_e = ps.E > 0 ? static_cast<int>(std::log2(static_cast<double>(ps.E))) : 0;
   const double mean_instr = ps.E > 0 ? static_cast<double>(ps.n_instr) / ps.E : 0.0;
   std::ostringstream k;
-  const bool prot = ps.n_instr > 0 &&
-                    static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr;
+  const bool prot = protected_profile(ps);
   k << ctx->device_name << "|V" << ctx->V << "|N" << lg_n << "|E" << lg_e << "|I"
     << static_cast<int>(std::lround(std::log2(1.0 + mean_instr) * 4.0)) << "|S" << ps.smax
     << "|P" << (prot ? sr::kOpsProtected : sr::kOpsAll);
@@ -418,8 +421,14 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
       SR_TRY(autotune_main(ctx, key));
       it = ctx->tuned.find(key);
     }
-    const int tdpt = it != ctx->tuned.end() ? it->second.first : 8;
-    const int tw = it != ctx->tuned.end() ? it->second.second : 8;
+    // Untuned defaults, the shapes the autotuner picks on the evolution
+    // workloads: 8 datapoints x 8 warps for the protected profile; 4 x 16 for
+    // populations over every operator, whose larger dispatch switch fits the
+    // instruction cache better at 4 datapoints (150 -> 82 ms on 4,000
+    // all-operator expressions x 1M datapoints).
+    const bool prot = protected_profile(ps);
+    const int tdpt = it != ctx->tuned.end() ? it->second.first : (prot ? 8 : 4);
+    const int tw = it != ctx->tuned.end() ? it->second.second : (prot ? 8 : 16);
     if (dpt == 0) dpt = tdpt;
     if (W == 0) W = tw;
   }
@@ -1852,6 +1861,9 @@ sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
   ps.sfu_per_dp = 0.0;
   ps.fp32_per_dp = 0.0;
   ctx->prep_stats.host_compile_time_ms = now_ms() - t0;
+  // No timing here: a generation loop would re-tune whenever its populations
+  // move to another shape class; the tuned shape of a class is used when the
+  // context has one, else the profile's default.
   SR_TRY(prepare_main_shape(ctx, false));
   ctx->prep_stats.node_evals = n_tok * ctx->N;
   ctx->prep_stats.node_evals_executed = ctx->prep_stats.node_evals;

@@ -342,7 +342,9 @@ def test_operator_profiles_give_identical_results():
     base = [prot.depth_tree(6, full=False) for _ in range(400)]
     base += [mixed.depth_tree(4, full=False) for _ in range(8)]   # a few rare operators
     extra = [rare.depth_tree(6, full=False) for _ in range(600)]
-    with sg.Evaluator(device=0) as ev:
+    # one launch shape for both (the untuned default shape depends on the
+    # profile, and the shape sets the summation order)
+    with sg.Evaluator(device=0, dpt=8, warps_per_block=8) as ev:
         ev.set_data(X)
         a = ev.eval_mse(Population.from_lists(base))
         b = ev.eval_mse(Population.from_lists(base + extra))[:len(base)]
