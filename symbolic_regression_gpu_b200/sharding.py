@@ -263,7 +263,10 @@ class DatapointShardedEvaluator:
         self.ev.set_data(np.ascontiguousarray(recv.cpu().numpy()[:, :n]))
 
     def eval_mse(self, pop: Population) -> np.ndarray:
-        """MSE of every expression over all shards' datapoints, on every rank."""
+        """MSE of every expression over all shards' datapoints, on every rank
+        (every rank passes the same population)."""
+        if pop.num_exprs == 0:
+            return np.empty(0, np.float32)
         s, c = self.ev.eval_sums(pop)
         g = _gather_rows(np.concatenate([np.asarray(s, np.float64), np.asarray(c, np.float64)]),
                          self.group, self.device)
@@ -272,6 +275,8 @@ class DatapointShardedEvaluator:
 
     def eval_grad(self, pop: Population):
         """(MSE [E], d MSE / d constants [C]) over all shards' datapoints."""
+        if pop.num_exprs == 0:
+            return np.empty(0, np.float32), np.empty(0, np.float32)
         self.ev.eval_grad(pop)
         s, c = self.ev.read_sums()
         gs = self.ev.read_grad_sums()

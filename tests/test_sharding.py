@@ -184,6 +184,8 @@ def _dp_rank_main(rank, world, port, tokens, values, offsets, X, out_dir, scatte
         mse, grad = sev.eval_grad(pop)
         np.save(os.path.join(out_dir, f"dgmse{rank}.npy"), mse)
         np.save(os.path.join(out_dir, f"dgrad{rank}.npy"), grad)
+        empty = Population(np.zeros(0, np.int32), np.zeros(0), np.zeros(1, np.int64))
+        assert sev.eval_mse(empty).size == 0
     finally:
         dist.destroy_process_group()
 
