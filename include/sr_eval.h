@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define SR_ABI_VERSION 1
+#define SR_ABI_VERSION 2
 
 /* ---- token encoding (reference src/utils/opcodes.h:10-40) ---------------- */
 #define SR_TOK_CONST 0
@@ -126,6 +126,11 @@ typedef struct sr_options {
                                subtrees on the device (same result)           */
   const char *tune_cache_path; /* JSON file for tuned shapes; NULL = none      */
   void *stream;             /* cudaStream_t to run on; NULL = own stream      */
+  int32_t smem_spill_slots; /* spill slots per warp kept in shared memory (the
+                               deeper ones live in per-warp global scratch):
+                               -1 = tuned / the default for the datapoints per
+                               thread, 0..16 = fixed                          */
+  int32_t reserved1;
 } sr_options;
 
 /* A population in CSR form: expression i is tokens/values[offsets[i] ..

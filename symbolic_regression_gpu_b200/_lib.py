@@ -60,6 +60,8 @@ class sr_options(Structure):
         ("device_detect", c_int32),
         ("tune_cache_path", c_char_p),
         ("stream", c_void_p),
+        ("smem_spill_slots", c_int32),
+        ("reserved1", c_int32),
     ]
 
 

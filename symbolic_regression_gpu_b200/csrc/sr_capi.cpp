@@ -195,7 +195,9 @@ bool protected_profile(const ProgramSet &ps) {
 }
 
 // Launch shape: groups of G cost-sorted expressions x spans of datapoints.
-sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
+// `split`: spill slots per warp kept in shared memory (-1 = the default for
+// the dpt); the deeper slots live in per-warp global scratch.
+sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, int split = -1,
                    int span_target = 1024, int per_warp = 4) {
   sr::Plan p;
   p.dpt = dpt;
@@ -203,7 +205,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W,
   p.ops = (!pred && protected_profile(ps)) ? sr::kOpsProtected : sr::kOpsAll;
   p.cache = !pred && ps.cache_refs;
   p.smax = std::max(ps.smax, 0);
-  p.s_smem = std::min(p.smax, sr::smem_spill_slots(dpt));
+  p.s_smem = std::min(p.smax, split < 0 ? sr::smem_spill_slots(dpt) : split);
   const int64_t tile = 32 * dpt;
   const int E = ps.E;
   p.G = std::max(1, W * per_warp);
@@ -349,7 +351,7 @@ void load_tune_cache(sr_context *ctx) {
   if (!ctx->opts.tune_cache_path) return;
   std::ifstream f(ctx->opts.tune_cache_path);
   if (!f) return;
-  // Format: one entry per line:  "key": [dpt, W],
+  // Format: one entry per line:  "key": [dpt, W, split],  (split optional)
   std::string line;
   while (std::getline(f, line)) {
     const size_t q0 = line.find('"'), q1 = line.find('"', q0 + 1);
@@ -357,11 +359,11 @@ void load_tune_cache(sr_context *ctx) {
     if (q0 == std::string::npos || q1 == std::string::npos || b0 == std::string::npos ||
         b1 == std::string::npos)
       continue;
-    int dpt = 0, w = 0;
-    if (std::sscanf(line.c_str() + b0, "[%d, %d]", &dpt, &w) == 2 &&
-        (dpt == 4 || dpt == 8 || dpt == 16) &&
-        w >= 1 && w <= sr::kMaxWarps)
-      ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w};
+    int dpt = 0, w = 0, split = -1;
+    const int n = std::sscanf(line.c_str() + b0, "[%d, %d, %d]", &dpt, &w, &split);
+    if (n >= 2 && (dpt == 4 || dpt == 8 || dpt == 16) && w >= 1 && w <= sr::kMaxWarps &&
+        split >= -1 && split <= sr::kMaxSpillSlots)
+      ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w, n == 3 ? split : -1};
   }
 }
 
@@ -372,47 +374,82 @@ void save_tune_cache(const sr_context *ctx) {
   f << "{\n";
   size_t i = 0;
   for (const auto &kv : ctx->tuned) {
-    f << "  \"" << kv.first << "\": [" << kv.second.first << ", " << kv.second.second << "]"
+    f << "  \"" << kv.first << "\": [" << kv.second.dpt << ", " << kv.second.W << ", "
+      << kv.second.split << "]"
       << (++i < ctx->tuned.size() ? "," : "") << "\n";
   }
   f << "}\n";
 }
 
-// Times each candidate shape on the prepared population and keeps the fastest.
+// Milliseconds of two launches of the prepared main set in the given shape
+// (after one warm-up launch); a negative value when the shape does not fit.
+static sr_status time_shape(sr_context *ctx, int dpt, int W, int split, float *ms_out) {
+  *ms_out = -1.f;
+  if (plan_set(ctx, ctx->main, false, dpt, W, split) != SR_OK) {
+    ctx->last_error.clear();
+    return SR_OK;
+  }
+  SR_TRY(upload_groups(ctx, ctx->main));
+  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(std::max<int64_t>(
+                       static_cast<int64_t>(ctx->main.plan.n_spans) * ctx->main.E, 1))));
+  cudaEvent_t a = ctx->ev[4], b = ctx->ev[5];
+  float t_sum = 0.f;
+  for (int rep = 0; rep < 3; ++rep) {
+    SR_TRY_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+    SR_TRY(launch_set(ctx, ctx->main, false, ctx->d_counter, nullptr, 0, nullptr));
+    SR_TRY_CUDA(ctx, cudaEventRecord(b, ctx->stream));
+    SR_TRY_CUDA(ctx, cudaEventSynchronize(b));
+    const float ms = elapsed_ms(a, b);
+    if (rep > 0) t_sum += ms;  // the first run warms up
+  }
+  *ms_out = t_sum;
+  return SR_OK;
+}
+
+// Times candidate shapes on the prepared population and keeps the fastest:
+// first datapoints per thread x warps per block with the default spill split,
+// then, for programs that spill, other splits of the spill slots between
+// shared memory and global scratch for the winning shape (fewer slots in
+// shared memory can fit more blocks per SM; more keep the deeper slots out
+// of L2).
 sr_status autotune_main(sr_context *ctx, const std::string &key) {
   SR_TRACE("sr: autotune");
   static const int kCand[][2] = {{16, 8}, {16, 16}, {8, 8}, {8, 16}, {4, 8}, {4, 16}};
   float best = 1e30f;
-  int best_dpt = 8, best_w = 8;
-  cudaEvent_t a = ctx->ev[4], b = ctx->ev[5];
+  sr_context::TunedShape win{8, 8, -1};
   for (const auto &c : kCand) {
-    if (plan_set(ctx, ctx->main, false, c[0], c[1]) != SR_OK) continue;
-    SR_TRY(upload_groups(ctx, ctx->main));
-    SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(std::max<int64_t>(
-                         static_cast<int64_t>(ctx->main.plan.n_spans) * ctx->main.E, 1))));
-    float t_sum = 0.f;
-    for (int rep = 0; rep < 3; ++rep) {
-      SR_TRY_CUDA(ctx, cudaEventRecord(a, ctx->stream));
-      SR_TRY(launch_set(ctx, ctx->main, false, ctx->d_counter, nullptr, 0, nullptr));
-      SR_TRY_CUDA(ctx, cudaEventRecord(b, ctx->stream));
-      SR_TRY_CUDA(ctx, cudaEventSynchronize(b));
-      const float ms = elapsed_ms(a, b);
-      if (rep > 0) t_sum += ms;  // first run warms up
-    }
-    if (t_sum < best) {
-      best = t_sum;
-      best_dpt = c[0];
-      best_w = c[1];
+    float ms = 0.f;
+    SR_TRY(time_shape(ctx, c[0], c[1], -1, &ms));
+    if (ms >= 0.f && ms < best) {
+      best = ms;
+      win = {c[0], c[1], -1};
     }
   }
-  ctx->tuned[key] = {best_dpt, best_w};
+  const int smax = ctx->main.smax;
+  if (smax > 0) {
+    const int rule = std::min(smax, sr::smem_spill_slots(win.dpt));
+    int tried[4] = {rule, -1, -1, -1};
+    int n_tried = 1;
+    for (const int split : {0, rule / 2, smax}) {
+      if (split > sr::kMaxSpillSlots || std::find(tried, tried + n_tried, split) != tried + n_tried)
+        continue;
+      tried[n_tried++] = split;
+      float ms = 0.f;
+      SR_TRY(time_shape(ctx, win.dpt, win.W, split, &ms));
+      if (ms >= 0.f && ms < best) {
+        best = ms;
+        win.split = split;
+      }
+    }
+  }
+  ctx->tuned[key] = win;
   save_tune_cache(ctx);
   return SR_OK;
 }
 
 sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
   ProgramSet &ps = ctx->main;
-  int dpt = ctx->opts.dpt, W = ctx->opts.warps_per_block;
+  int dpt = ctx->opts.dpt, W = ctx->opts.warps_per_block, split = -1;
   if (dpt == 0 || W == 0) {
     if (!ctx->tune_loaded) load_tune_cache(ctx);
     const std::string key = tune_key(ctx, ps);
@@ -427,12 +464,16 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
     // instruction cache better at 4 datapoints (150 -> 82 ms on 4,000
     // all-operator expressions x 1M datapoints).
     const bool prot = protected_profile(ps);
-    const int tdpt = it != ctx->tuned.end() ? it->second.first : (prot ? 8 : 4);
-    const int tw = it != ctx->tuned.end() ? it->second.second : (prot ? 8 : 16);
+    const bool have = it != ctx->tuned.end();
+    const int tdpt = have ? it->second.dpt : (prot ? 8 : 4);
+    const int tw = have ? it->second.W : (prot ? 8 : 16);
+    // the tuned split belongs to the tuned shape only
+    if (have && (dpt == 0 || dpt == tdpt) && (W == 0 || W == tw)) split = it->second.split;
     if (dpt == 0) dpt = tdpt;
     if (W == 0) W = tw;
   }
-  SR_TRY(plan_set(ctx, ps, false, dpt, W));
+  if (ctx->opts.smem_spill_slots >= 0) split = ctx->opts.smem_spill_slots;
+  SR_TRY(plan_set(ctx, ps, false, dpt, W, split));
   SR_TRY(upload_groups(ctx, ps));
   SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
                        std::max<int64_t>(static_cast<int64_t>(ps.plan.n_spans) * ps.E, 1))));
@@ -518,6 +559,7 @@ sr_status sr_options_init(sr_options *o) {
   o->host_threads = 0;
   o->tune_cache_path = nullptr;
   o->stream = nullptr;
+  o->smem_spill_slots = -1;
   return SR_OK;
 }
 
@@ -529,6 +571,8 @@ sr_status sr_create(const sr_options *opts, sr_context **out) {
   else sr_options_init(&o);
   if (o.dpt != 0 && o.dpt != 4 && o.dpt != 8 && o.dpt != 16) return SR_ERR_INVALID_ARGUMENT;
   if (o.warps_per_block < 0 || o.warps_per_block > sr::kMaxWarps) return SR_ERR_INVALID_ARGUMENT;
+  if (o.smem_spill_slots < -1 || o.smem_spill_slots > sr::kMaxSpillSlots)
+    return SR_ERR_INVALID_ARGUMENT;
   if (o.cache_capacity < 0 || o.min_subtree_size < 1 || o.min_subtree_freq < 1)
     return SR_ERR_INVALID_ARGUMENT;
   int ndev = 0;

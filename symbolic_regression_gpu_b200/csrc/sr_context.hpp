@@ -275,8 +275,12 @@ struct sr_context {
   // statistics of the prepared population
   sr_stats prep_stats{};
 
-  // tuned launch shapes: key -> (dpt, W)
-  std::map<std::string, std::pair<int, int>> tuned;
+  // tuned launch shapes: key -> (dpt, W, spill slots in shared memory; -1 =
+  // the default for the dpt)
+  struct TunedShape {
+    int dpt, W, split;
+  };
+  std::map<std::string, TunedShape> tuned;
   bool tune_loaded = false;
 
   sr_status fail(sr_status s, const std::string &msg) {

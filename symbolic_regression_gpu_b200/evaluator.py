@@ -36,7 +36,7 @@ class Evaluator:
                  min_subtree_size: int = 3, min_subtree_freq: int = 10, dpt: int = 0,
                  warps_per_block: int = 0, autotune: bool = False, host_threads: int = 0,
                  tune_cache_path: Optional[str] = None, stream=None, use_graphs: bool = False,
-                 device_detect: bool = False):
+                 device_detect: bool = False, smem_spill_slots: int = -1):
         opts = _lib.sr_options()
         _lib.check(_lib.lib.sr_options_init(ctypes.byref(opts)))
         self.device = device
@@ -50,6 +50,7 @@ class Evaluator:
         opts.use_graphs = 1 if use_graphs else 0
         opts.device_detect = 1 if device_detect else 0
         opts.host_threads = host_threads
+        opts.smem_spill_slots = smem_spill_slots
         self._tune_path = tune_cache_path.encode() if tune_cache_path else None
         opts.tune_cache_path = self._tune_path
         if stream is not None:

@@ -50,7 +50,7 @@ def test_reference_cpp_entry_points_exported():
 
 def test_abi_version_and_status_strings():
     from symbolic_regression_gpu_b200 import _lib
-    assert _lib.lib.sr_abi_version() == 1
+    assert _lib.lib.sr_abi_version() == 2
     for s in range(13):
         assert _lib.status_string(s) not in ("", "unknown status")
 

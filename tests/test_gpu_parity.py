@@ -350,3 +350,45 @@ def test_operator_profiles_give_identical_results():
         b = ev.eval_mse(Population.from_lists(base + extra))[:len(base)]
     same = (a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))
     assert same.all()
+
+
+@pytest.mark.parametrize("split", [0, 2, 7])
+def test_spill_split_gives_identical_results(split):
+    """Spill slots kept in shared memory or in global scratch (the split the
+    autotuner chooses) hold the same values: identical MSE bits."""
+    rng = np.random.default_rng(5)
+    V, N = 3, 20_000
+    X = np.empty((V + 1, N), np.float32)
+    X[:V] = rng.uniform(-2, 2, size=(V, N))
+    X[V] = X[0] * X[1] - X[2]
+    gen = synth.TreeGen(rng, V, binary=(1, 2, 3, 8), unary=(10, 11), p_const=0.3, p_unary=0.0)
+    pop = Population.from_lists([gen.depth_tree(8, full=True) for _ in range(48)]
+                                + [gen.depth_tree(5, full=False) for _ in range(200)])
+    with sg.Evaluator(device=0, dpt=8, warps_per_block=8) as ev:
+        ev.set_data(X)
+        want = ev.eval_mse(pop)
+    with sg.Evaluator(device=0, dpt=8, warps_per_block=8, smem_spill_slots=split) as ev:
+        ev.set_data(X)
+        got = ev.eval_mse(pop)
+    assert ((got.view(np.uint32) == want.view(np.uint32)) | (np.isnan(got) & np.isnan(want))).all()
+
+
+def test_autotuner_records_the_spill_split(tmp_path):
+    rng = np.random.default_rng(6)
+    V, N = 3, 50_000
+    X = rng.uniform(-2, 2, size=(V + 1, N)).astype(np.float32)
+    gen = synth.TreeGen(rng, V, binary=(1, 2, 3, 8), unary=(10, 11), p_const=0.3, p_unary=0.0)
+    pop = Population.from_lists([gen.depth_tree(7, full=True) for _ in range(300)])
+    path = tmp_path / "tune.json"
+    with sg.Evaluator(device=0, autotune=True, tune_cache_path=str(path)) as ev:
+        ev.set_data(X)
+        a = ev.eval_mse(pop)
+    entries = [ln for ln in path.read_text().splitlines() if ln.strip().startswith('"')]
+    assert len(entries) == 1
+    shape = [int(x) for x in entries[0].split("[")[1].split("]")[0].split(",")]
+    assert len(shape) == 3 and shape[0] in (4, 8, 16) and -1 <= shape[2] <= 16
+    # a new context reads the tuned shape back and gives the same result
+    with sg.Evaluator(device=0, autotune=True, tune_cache_path=str(path)) as ev:
+        ev.set_data(X)
+        b = ev.eval_mse(pop)
+    assert ((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))).all()
