@@ -196,9 +196,11 @@ bool protected_profile(const ProgramSet &ps) {
 
 // Launch shape: groups of G cost-sorted expressions x spans of datapoints.
 // `split`: spill slots per warp kept in shared memory (-1 = the default for
-// the dpt); the deeper slots live in per-warp global scratch.
+// the dpt); the deeper slots live in per-warp global scratch.  `per_warp`:
+// expressions per group and evaluating warp (a group of G = W x per_warp
+// expressions shares each staged X span).
 sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, int split = -1,
-                   int span_target = 1024, int per_warp = 4) {
+                   int per_warp = 4, int span_target = 1024) {
   sr::Plan p;
   p.dpt = dpt;
   p.W = W;
@@ -230,10 +232,8 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
   // sized against the device's memory (the allocation itself reports
   // SR_ERR_OUT_OF_MEMORY when the free memory is short).
   if (!pred) {
-    size_t free_b = 0, total_b = 0;
-    SR_TRY_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b));
     const double need = static_cast<double>(p.n_spans) * E * 16.0;
-    if (need > 0.9 * static_cast<double>(total_b))
+    if (need > 0.9 * static_cast<double>(ctx->device_memory))
       return ctx->fail(SR_ERR_UNSUPPORTED,
                        "partial-sum buffer (" + std::to_string(static_cast<int64_t>(need)) +
                            " bytes) exceeds the device memory; split the population or the "
@@ -351,7 +351,8 @@ void load_tune_cache(sr_context *ctx) {
   if (!ctx->opts.tune_cache_path) return;
   std::ifstream f(ctx->opts.tune_cache_path);
   if (!f) return;
-  // Format: one entry per line:  "key": [dpt, W, split],  (split optional)
+  // Format: one entry per line:  "key": [dpt, W, split, per_warp],  (the last
+  // two optional)
   std::string line;
   while (std::getline(f, line)) {
     const size_t q0 = line.find('"'), q1 = line.find('"', q0 + 1);
@@ -359,11 +360,12 @@ void load_tune_cache(sr_context *ctx) {
     if (q0 == std::string::npos || q1 == std::string::npos || b0 == std::string::npos ||
         b1 == std::string::npos)
       continue;
-    int dpt = 0, w = 0, split = -1;
-    const int n = std::sscanf(line.c_str() + b0, "[%d, %d, %d]", &dpt, &w, &split);
+    int dpt = 0, w = 0, split = -1, per_warp = 4;
+    const int n = std::sscanf(line.c_str() + b0, "[%d, %d, %d, %d]", &dpt, &w, &split, &per_warp);
     if (n >= 2 && (dpt == 4 || dpt == 8 || dpt == 16) && w >= 1 && w <= sr::kMaxWarps &&
-        split >= -1 && split <= sr::kMaxSpillSlots)
-      ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w, n == 3 ? split : -1};
+        split >= -1 && split <= sr::kMaxSpillSlots && per_warp >= 1 && per_warp <= 16)
+      ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w, n >= 3 ? split : -1,
+                                                       n >= 4 ? per_warp : 4};
   }
 }
 
@@ -375,7 +377,7 @@ void save_tune_cache(const sr_context *ctx) {
   size_t i = 0;
   for (const auto &kv : ctx->tuned) {
     f << "  \"" << kv.first << "\": [" << kv.second.dpt << ", " << kv.second.W << ", "
-      << kv.second.split << "]"
+      << kv.second.split << ", " << kv.second.per_warp << "]"
       << (++i < ctx->tuned.size() ? "," : "") << "\n";
   }
   f << "}\n";
@@ -383,9 +385,10 @@ void save_tune_cache(const sr_context *ctx) {
 
 // Milliseconds of two launches of the prepared main set in the given shape
 // (after one warm-up launch); a negative value when the shape does not fit.
-static sr_status time_shape(sr_context *ctx, int dpt, int W, int split, float *ms_out) {
+static sr_status time_shape(sr_context *ctx, int dpt, int W, int split, int per_warp,
+                            float *ms_out) {
   *ms_out = -1.f;
-  if (plan_set(ctx, ctx->main, false, dpt, W, split) != SR_OK) {
+  if (plan_set(ctx, ctx->main, false, dpt, W, split, per_warp) != SR_OK) {
     ctx->last_error.clear();
     return SR_OK;
   }
@@ -411,18 +414,19 @@ static sr_status time_shape(sr_context *ctx, int dpt, int W, int split, float *m
 // then, for programs that spill, other splits of the spill slots between
 // shared memory and global scratch for the winning shape (fewer slots in
 // shared memory can fit more blocks per SM; more keep the deeper slots out
-// of L2).
+// of L2), then the expressions per group (2, 4 or 8 per warp: larger groups
+// reuse each staged X span more, smaller ones balance better).
 sr_status autotune_main(sr_context *ctx, const std::string &key) {
   SR_TRACE("sr: autotune");
   static const int kCand[][2] = {{16, 8}, {16, 16}, {8, 8}, {8, 16}, {4, 8}, {4, 16}};
   float best = 1e30f;
-  sr_context::TunedShape win{8, 8, -1};
+  sr_context::TunedShape win{8, 8, -1, 4};
   for (const auto &c : kCand) {
     float ms = 0.f;
-    SR_TRY(time_shape(ctx, c[0], c[1], -1, &ms));
+    SR_TRY(time_shape(ctx, c[0], c[1], -1, 4, &ms));
     if (ms >= 0.f && ms < best) {
       best = ms;
-      win = {c[0], c[1], -1};
+      win = {c[0], c[1], -1, 4};
     }
   }
   const int smax = ctx->main.smax;
@@ -435,11 +439,19 @@ sr_status autotune_main(sr_context *ctx, const std::string &key) {
         continue;
       tried[n_tried++] = split;
       float ms = 0.f;
-      SR_TRY(time_shape(ctx, win.dpt, win.W, split, &ms));
+      SR_TRY(time_shape(ctx, win.dpt, win.W, split, 4, &ms));
       if (ms >= 0.f && ms < best) {
         best = ms;
         win.split = split;
       }
+    }
+  }
+  for (const int per_warp : {2, 8}) {
+    float ms = 0.f;
+    SR_TRY(time_shape(ctx, win.dpt, win.W, win.split, per_warp, &ms));
+    if (ms >= 0.f && ms < best) {
+      best = ms;
+      win.per_warp = per_warp;
     }
   }
   ctx->tuned[key] = win;
@@ -449,7 +461,7 @@ sr_status autotune_main(sr_context *ctx, const std::string &key) {
 
 sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
   ProgramSet &ps = ctx->main;
-  int dpt = ctx->opts.dpt, W = ctx->opts.warps_per_block, split = -1;
+  int dpt = ctx->opts.dpt, W = ctx->opts.warps_per_block, split = -1, per_warp = 4;
   if (dpt == 0 || W == 0) {
     if (!ctx->tune_loaded) load_tune_cache(ctx);
     const std::string key = tune_key(ctx, ps);
@@ -468,12 +480,15 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
     const int tdpt = have ? it->second.dpt : (prot ? 8 : 4);
     const int tw = have ? it->second.W : (prot ? 8 : 16);
     // the tuned split belongs to the tuned shape only
-    if (have && (dpt == 0 || dpt == tdpt) && (W == 0 || W == tw)) split = it->second.split;
+    if (have && (dpt == 0 || dpt == tdpt) && (W == 0 || W == tw)) {
+      split = it->second.split;
+      per_warp = it->second.per_warp;
+    }
     if (dpt == 0) dpt = tdpt;
     if (W == 0) W = tw;
   }
   if (ctx->opts.smem_spill_slots >= 0) split = ctx->opts.smem_spill_slots;
-  SR_TRY(plan_set(ctx, ps, false, dpt, W, split));
+  SR_TRY(plan_set(ctx, ps, false, dpt, W, split, per_warp));
   SR_TRY(upload_groups(ctx, ps));
   SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
                        std::max<int64_t>(static_cast<int64_t>(ps.plan.n_spans) * ps.E, 1))));
@@ -593,6 +608,7 @@ sr_status sr_create(const sr_options *opts, sr_context **out) {
     return SR_ERR_NO_DEVICE;  // this build carries sm_100a code only
   }
   ctx->num_sms = prop.multiProcessorCount;
+  ctx->device_memory = prop.totalGlobalMem;
   ctx->device_name = prop.name;
   ctx->cache.capacity = o.cache_capacity;
   cudaError_t e = cudaSuccess;

@@ -209,6 +209,7 @@ struct sr_context {
   sr_options opts{};
   int device = 0;
   int num_sms = 0;
+  size_t device_memory = 0;  // bytes of device memory (cudaDeviceProp::totalGlobalMem)
   std::string device_name;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -275,10 +276,10 @@ struct sr_context {
   // statistics of the prepared population
   sr_stats prep_stats{};
 
-  // tuned launch shapes: key -> (dpt, W, spill slots in shared memory; -1 =
-  // the default for the dpt)
+  // tuned launch shapes: key -> (dpt, W, spill slots in shared memory (-1 =
+  // the default for the dpt), expressions per group and warp)
   struct TunedShape {
-    int dpt, W, split;
+    int dpt, W, split, per_warp;
   };
   std::map<std::string, TunedShape> tuned;
   bool tune_loaded = false;

@@ -386,7 +386,8 @@ def test_autotuner_records_the_spill_split(tmp_path):
     entries = [ln for ln in path.read_text().splitlines() if ln.strip().startswith('"')]
     assert len(entries) == 1
     shape = [int(x) for x in entries[0].split("[")[1].split("]")[0].split(",")]
-    assert len(shape) == 3 and shape[0] in (4, 8, 16) and -1 <= shape[2] <= 16
+    assert len(shape) == 4 and shape[0] in (4, 8, 16) and -1 <= shape[2] <= 16
+    assert shape[3] in (2, 4, 8)
     # a new context reads the tuned shape back and gives the same result
     with sg.Evaluator(device=0, autotune=True, tune_cache_path=str(path)) as ev:
         ev.set_data(X)
