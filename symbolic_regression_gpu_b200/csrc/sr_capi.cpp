@@ -1093,7 +1093,13 @@ static sr_status enqueue_launch(sr_context *ctx, int *launches_out) {
   return SR_OK;
 }
 
-sr_status sr_launch(sr_context *ctx) {
+static sr_status launch_prepared(sr_context *ctx, bool allow_graph);
+
+sr_status sr_launch(sr_context *ctx) { return launch_prepared(ctx, true); }
+
+// allow_graph = false for one-shot evaluations (a graph pays off only when the
+// prepared launch is replayed).
+static sr_status launch_prepared(sr_context *ctx, bool allow_graph) {
   SR_TRACE("sr_launch");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   if (ctx->E == 0) return SR_OK;
@@ -1101,7 +1107,7 @@ sr_status sr_launch(sr_context *ctx) {
   DeviceScope scope(ctx->device);
   cudaStream_t s = ctx->stream;
   int launches = 0;
-  if (ctx->opts.use_graphs) {
+  if (ctx->opts.use_graphs && (allow_graph || ctx->graph_exec)) {
     if (!ctx->graph_exec) {
       // Relaxed mode: the launchers set kernel attributes while capturing.
       SR_TRY_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
@@ -1278,7 +1284,7 @@ sr_status sr_eval_mse(sr_context *ctx, const sr_population *pop, uint32_t flags,
     if (stats) *stats = sr_stats{};
     return SR_OK;
   }
-  SR_TRY(sr_launch(ctx));
+  SR_TRY(launch_prepared(ctx, false));
   SR_TRY(sr_read_mse(ctx, mse_out, stats));
   if (stats) stats->total_eval_time_ms = now_ms() - t0;
   return SR_OK;
