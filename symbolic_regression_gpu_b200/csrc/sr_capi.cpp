@@ -1,5 +1,8 @@
 // sr_capi.cpp — the C ABI (sr_eval.h): context lifecycle, dataset upload,
-// population compilation / planning / upload, launches and read-back.
+// population compilation / planning / upload, launches and read-back
+// (gradients and Adam: sr_capi_grad.cpp; the FP64 reference, the device
+// generation loop, microbenchmarks, detection and host-only helpers:
+// sr_capi_tools.cpp; shared helpers: sr_capi_internal.hpp).
 //
 // Reference counterpart: evaluate_gpu_mse (src/cleaned/cl_gpu_eval.cu:332-564)
 // and evaluate_gpu_simple (src/cleaned/cl_gpu_simple.cu:187-310).  Where the
@@ -20,6 +23,7 @@
 #include <thread>
 
 #include "sr_adjoint.hpp"
+#include "sr_capi_internal.hpp"
 #include "sr_context.hpp"
 #include "sr_detect_gpu.hpp"
 #include "sr_evolve.hpp"
@@ -28,8 +32,10 @@
 
 using sr::Instr;
 using sr::ProgramSet;
+using namespace sr::capi;
 
-namespace {
+namespace sr {
+namespace capi {
 
 double now_ms() {
   using namespace std::chrono;
@@ -54,31 +60,6 @@ sr_status cuda_fail(sr_context *ctx, cudaError_t e, const char *what) {
   cudaGetLastError();  // reported here; a non-sticky error must not fail the next call's launch check
   return ctx->fail(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define SR_TRY_CUDA(ctx, call)                              \
-  do {                                                      \
-    const cudaError_t e_ = (call);                          \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
-  } while (0)
-
-#define SR_TRY(call)                  \
-  do {                                \
-    const sr_status s_ = (call);      \
-    if (s_ != SR_OK) return s_;       \
-  } while (0)
-
-// Makes ctx->device current for the scope of an API call.
-struct DeviceScope {
-  int prev = -1;
-  explicit DeviceScope(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceScope() {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 int host_threads(const sr_context *ctx) {
   int t = ctx->opts.host_threads;
@@ -199,8 +180,8 @@ bool protected_profile(const ProgramSet &ps) {
 // the dpt); the deeper slots live in per-warp global scratch.  `per_warp`:
 // expressions per group and evaluating warp (a group of G = W x per_warp
 // expressions shares each staged X span).
-sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, int split = -1,
-                   int per_warp = 4, int span_target = 1024) {
+sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, int split,
+                   int per_warp, int span_target) {
   sr::Plan p;
   p.dpt = dpt;
   p.W = W;
@@ -495,21 +476,22 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
   return SR_OK;
 }
 
-}  // namespace
+}  // namespace capi
+}  // namespace sr
 
 // ============================================================================
 // Record timing event k on the context stream.  While sr_launch captures a
 // graph the event is recorded as an external event, which makes it an
 // event-record node of the graph (a plain record would only mark a capture
 // dependency); outside capture that flag is not accepted.
-static cudaError_t record_event(sr_context *ctx, int k) {
+cudaError_t sr::capi::record_event(sr_context *ctx, int k) {
   return ctx->capturing ? cudaEventRecordWithFlags(ctx->ev[k], ctx->stream, cudaEventRecordExternal)
                         : cudaEventRecord(ctx->ev[k], ctx->stream);
 }
 
 // Forget the prepared launch (and its captured graph, whose kernel arguments
 // point into buffers that the next prepare / set_data may move).
-static void reset_prepared(sr_context *ctx) {
+void sr::capi::reset_prepared(sr_context *ctx) {
   ctx->mode = sr::Mode::kNone;
   ctx->cache.rollback();  // subtrees of a launch that never ran hold no values
   if (ctx->graph_exec) {
@@ -520,7 +502,7 @@ static void reset_prepared(sr_context *ctx) {
 }
 
 // Drop the dataset, the cache built on it and every prepared launch.
-static void invalidate_data(sr_context *ctx) {
+void sr::capi::invalidate_data(sr_context *ctx) {
   reset_prepared(ctx);
   ctx->cache.clear();  // cached subtree values belong to the old data
   ctx->V = -1;
@@ -725,9 +707,14 @@ sr_status sr_set_data_rows(sr_context *ctx, const float *const *rows, int32_t nu
   return set_data_host(ctx, nullptr, rows, num_vars, num_dps);
 }
 
+}  // extern "C"
+
+namespace sr {
+namespace capi {
+
 // ---- prepare --------------------------------------------------------------
 
-static sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
+sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
   SR_TRACE("sr: prepare plain");
   sr::PlainSet &ps = ctx->plain;
   const int E = pop->num_exprs;
@@ -800,7 +787,7 @@ static sr_status prepare_plain(sr_context *ctx, const sr_population *pop) {
 
 // Common-subtree detection on the context's GPU: the same Detection as
 // sr::detect_common_subtrees (groups largest first, stable in hash order).
-static sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, const double *val,
+sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, const double *val,
                                   const int64_t *off, int min_size, int min_freq,
                                   sr::Detection &out) {
   SR_TRACE("sr: detect (device)");
@@ -909,7 +896,7 @@ static sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, co
   return SR_OK;
 }
 
-static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint32_t flags) {
+sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint32_t flags) {
   SR_TRACE("sr: prepare cached");
   const int E = pop->num_exprs;
   const int64_t T = pop->offsets[E];
@@ -1006,12 +993,8 @@ static sr_status prepare_cached(sr_context *ctx, const sr_population *pop, uint3
   return SR_OK;
 }
 
-}  // extern "C"
-
-namespace {
-sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute);
-sr_status launch_grad(sr_context *ctx);
-}  // namespace
+}  // namespace capi
+}  // namespace sr
 
 extern "C" {
 
@@ -1138,7 +1121,12 @@ static sr_status launch_prepared(sr_context *ctx, bool allow_graph) {
   return SR_OK;
 }
 
-static sr_status check_device_error(sr_context *ctx) {
+}  // extern "C"
+
+namespace sr {
+namespace capi {
+
+sr_status check_device_error(sr_context *ctx) {
   if (*ctx->h_error == 0) return SR_OK;
   const int32_t code = *ctx->h_error;
   *ctx->h_error = 0;
@@ -1150,7 +1138,7 @@ static sr_status check_device_error(sr_context *ctx) {
   return ctx->fail(SR_ERR_DEVICE_CHECK, "device bounds check failed");
 }
 
-static void fill_stats(sr_context *ctx, sr_stats *st) {
+void fill_stats(sr_context *ctx, sr_stats *st) {
   if (!st) return;
   *st = ctx->prep_stats;
   if (ctx->timing_valid) {
@@ -1170,6 +1158,11 @@ static void fill_stats(sr_context *ctx, sr_stats *st) {
   st->blocks = p.blocks;
   st->work_items = static_cast<int32_t>(p.items());
 }
+
+}  // namespace capi
+}  // namespace sr
+
+extern "C" {
 
 sr_status sr_read_mse(sr_context *ctx, float *mse_out, sr_stats *stats) {
   SR_TRACE("sr_read_mse");
@@ -1344,832 +1337,3 @@ sr_status sr_count_constants(const sr_population *pop, int64_t *const_offsets) {
 }
 
 }  // extern "C"
-
-// ---- forward + adjoint ------------------------------------------------------
-
-namespace {
-
-constexpr int kMaxAdjConsts = 64;  // constants per expression with a gradient
-
-// Compile, lay out constants, split expressions into tape-length classes and
-// upload everything the adjoint launches need.
-sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute) {
-  sr::GradSet &g = ctx->grad;
-  g.recompute = recompute;
-  ProgramSet &ps = ctx->main;
-  const int E = pop->num_exprs;
-  SR_TRY(compile_set(ctx, E, pop->tokens, pop->values, pop->offsets, nullptr, ps));
-  SR_TRY(upload_code(ctx, ps));
-  // Constants: CSR offsets and the bytecode word that holds each one.
-  SR_TRY_CUDA(ctx, g.h_const_off.ensure(static_cast<size_t>(E) + 1));
-  SR_TRY_CUDA(ctx, g.h_const_cnt.ensure(static_cast<size_t>(std::max(E, 1))));
-  int64_t C = 0;
-  int gmax = 0;
-  for (int x = 0; x < E; ++x) {
-    const int nc = ps.n_const[static_cast<size_t>(x)];
-    if (nc > kMaxAdjConsts)
-      return ctx->fail(SR_ERR_UNSUPPORTED, "expression " + std::to_string(x) + " has " +
-                                               std::to_string(nc) + " constants (gradient limit " +
-                                               std::to_string(kMaxAdjConsts) + ")");
-    g.h_const_off.p[x] = C;
-    g.h_const_cnt.p[x] = nc;
-    C += nc;
-    gmax = std::max(gmax, nc);
-  }
-  g.h_const_off.p[E] = C;
-  g.C = C;
-  SR_TRY_CUDA(ctx, g.h_const_loc.ensure(static_cast<size_t>(std::max<int64_t>(C, 1))));
-  SR_TRY_CUDA(ctx, g.h_consts.ensure(static_cast<size_t>(std::max<int64_t>(C, 1))));
-  for (int x = 0; x < E; ++x) {
-    const int64_t i0 = ps.h_off.p[x];
-    const int64_t base = g.h_const_off.p[x];
-    for (int i = 0; i < ps.h_len.p[x]; ++i) {
-      const Instr &in = ps.h_code.p[i0 + i];
-      const uint32_t ca = in.c & 0x3FFu, cb = (in.c >> 10) & 0x3FFu;
-      if (sr::instr_load(in.w) && sr::instr_leaf_kind(in.w) == sr::kLeafC && ca != sr::kNoConst) {
-        g.h_const_loc.p[base + ca] = ((i0 + i) << 1);
-        std::memcpy(&g.h_consts.p[base + ca], &in.a, sizeof(float));
-      }
-      if (sr::instr_b_kind(in.w) == sr::kBC && cb != sr::kNoConst) {
-        g.h_const_loc.p[base + cb] = ((i0 + i) << 1) | 1;
-        std::memcpy(&g.h_consts.p[base + cb], &in.b, sizeof(float));
-      }
-    }
-  }
-  // Backward range and Jacobian-tape length of each program: the sweep runs
-  // from the last instruction down to the lowest one holding a constant
-  // (lo); the tape holds d out / d T of [lo, len) and d out / d b of the
-  // instructions in that range whose operand b is a constant or a spilled
-  // subtree.
-  SR_TRY_CUDA(ctx, g.h_bwd_lo.ensure(static_cast<size_t>(std::max(E, 1))));
-  std::vector<int32_t> tape_need(static_cast<size_t>(E));
-  for (int x = 0; x < E; ++x) {
-    const Instr *code = ps.h_code.p + ps.h_off.p[x];
-    const int len = ps.h_len.p[x];
-    int lo = len;
-    for (int i = 0; i < len; ++i) {
-      const Instr &in = code[i];
-      const bool leaf_c = sr::instr_load(in.w) && sr::instr_leaf_kind(in.w) == sr::kLeafC &&
-                          (in.c & 0x3FFu) != sr::kNoConst;
-      const bool b_c = sr::instr_b_kind(in.w) == sr::kBC && ((in.c >> 10) & 0x3FFu) != sr::kNoConst;
-      if (leaf_c || b_c) {
-        lo = i;
-        break;
-      }
-    }
-    int nb = 0;
-    for (int i = lo; i < len; ++i) {
-      const uint32_t bk = sr::instr_b_kind(code[i].w);
-      nb += (bk == sr::kBC || bk == sr::kBS) ? 1 : 0;
-    }
-    g.h_bwd_lo.p[x] = lo;
-    if (recompute) {
-      // Segment tape, adjoint spill slots, checkpoints.
-      const int seg = sr::adj_segment();
-      const int nseg = (len + seg - 1) / seg;
-      tape_need[static_cast<size_t>(x)] =
-          2 * std::min(seg, len) + ps.smax + std::max(nseg - 1, 0) * (1 + ps.smax);
-    } else {
-      tape_need[static_cast<size_t>(x)] = (len - lo) + nb;
-    }
-  }
-  // Tape-length classes, each a separate launch with its own tape size.
-  static const int kTapeClasses[] = {8, 16, 32, 64, 128, 256, 512, 2048};
-  constexpr int kNumClasses = 8;
-  std::vector<std::vector<int32_t>> members(kNumClasses);
-  for (int x = 0; x < E; ++x) {
-    const int need = tape_need[static_cast<size_t>(x)];
-    int k = 0;
-    while (k < kNumClasses - 1 && need > kTapeClasses[k]) ++k;
-    members[static_cast<size_t>(k)].push_back(x);
-  }
-  const int dpt = sr::adj_dpt();
-  const int64_t tile = 32 * dpt;
-  int dev_max_smem = 0;
-  cudaDeviceGetAttribute(&dev_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
-  // One span for every class (the MSE partials are laid out per span): the
-  // largest of 1024 / 512 / 256 / 128 datapoints whose double-buffered X
-  // stage fits in 48 KB.
-  int span = 1024;
-  while (span > tile && 2 * static_cast<int64_t>(ctx->V + 1) * span * 4 > 48 * 1024) span /= 2;
-  g.span = static_cast<int>(std::min<int64_t>(span, std::max<int64_t>(tile, round_up(ctx->N, tile))));
-  g.n_spans = (ctx->N == 0) ? 0 : static_cast<int>((ctx->N + g.span - 1) / g.span);
-  g.classes.clear();
-  std::vector<int32_t> table;
-  int64_t spill_floats = 0, gtape_floats = 0;
-  const int s_smem = std::min(ps.smax, sr::smem_spill_slots(dpt));
-  for (int k = 0; k < kNumClasses; ++k) {
-    auto &mem = members[static_cast<size_t>(k)];
-    if (mem.empty()) continue;
-    sr::AdjClass cl;
-    int tape_len = 1, cg = 0;
-    int maxlen = 1;
-    for (int32_t x : mem) {
-      tape_len = std::max(tape_len, tape_need[static_cast<size_t>(x)]);
-      cg = std::max(cg, ps.n_const[static_cast<size_t>(x)]);
-      maxlen = std::max(maxlen, static_cast<int>(ps.h_len.p[x]));
-    }
-    cl.seg_cap = std::min(sr::adj_segment(), maxlen);
-    cl.tape_len = tape_len;
-    cl.gmax = std::max(cg, 1);
-    // Most resident evaluating warps per SM.  A shared-memory tape costs
-    // occupancy (every warp holds its whole tape), a global one costs L2
-    // traffic (each tape entry is written and read back once per tile, by the
-    // same warp, so it stays in L2 while the resident tapes fit there): the
-    // global tape is taken only when it gives strictly more resident warps
-    // and the resident tapes stay within kL2TapeBytes.
-    constexpr int64_t kL2TapeBytes = 64ll << 20;
-    int best_w = 0, best_res = 0;
-    size_t best_smem = 0;
-    for (int pass = 0; pass < 2; ++pass) {
-      const bool gt = (pass == 1);
-      for (int W = sr::kMaxWarps; W >= 1; --W) {
-        const size_t smem =
-            sr::adj_smem_bytes(W, ctx->V, s_smem, g.span, cl.tape_len, cl.gmax, gt);
-        if (smem > static_cast<size_t>(dev_max_smem)) continue;
-        int bps = 0;
-        SR_TRY_CUDA(ctx, sr::adj_configure(smem, W, gt, recompute, &bps));
-        if (bps <= 0) continue;
-        const int64_t resident_tape =
-            static_cast<int64_t>(W) * bps * ctx->num_sms * cl.tape_len * tile * 4;
-        if (gt && best_w != 0 && resident_tape > kL2TapeBytes) continue;
-        if (W * bps > best_res) {
-          best_res = W * bps;
-          best_w = W;
-          best_smem = smem;
-          cl.global_tape = gt;
-        }
-      }
-    }
-    if (best_w == 0)
-      return ctx->fail(SR_ERR_UNSUPPORTED, "no adjoint launch shape fits " +
-                                               std::to_string(cl.tape_len) + " tape entries");
-    sr::Plan &p = cl.plan;
-    p.dpt = dpt;
-    p.W = best_w;
-    p.smax = ps.smax;
-    p.s_smem = s_smem;
-    p.G = best_w * 4;
-    p.n_groups = static_cast<int>((mem.size() + p.G - 1) / p.G);
-    p.span = g.span;
-    p.n_spans = g.n_spans;
-    p.smem = best_smem;
-    p.blocks = static_cast<int>(std::min<int64_t>(
-        static_cast<int64_t>(best_res / best_w) * ctx->num_sms, std::max<int64_t>(p.items(), 1)));
-    spill_floats = std::max<int64_t>(spill_floats, static_cast<int64_t>(p.blocks) * p.W *
-                                                       (p.smax - p.s_smem) * tile);
-    if (cl.global_tape)
-      gtape_floats = std::max<int64_t>(gtape_floats, static_cast<int64_t>(p.blocks) * p.W *
-                                                         cl.tape_len * tile);
-    std::stable_sort(mem.begin(), mem.end(), [&](int32_t a, int32_t b) {
-      return ps.cost[static_cast<size_t>(a)] > ps.cost[static_cast<size_t>(b)];
-    });
-    cl.group_off = static_cast<int64_t>(table.size());
-    for (int64_t q = 0; q < static_cast<int64_t>(p.n_groups) * p.G; ++q)
-      table.push_back(q < static_cast<int64_t>(mem.size()) ? mem[static_cast<size_t>(q)] : -1);
-    g.classes.push_back(cl);
-  }
-  // Uploads.
-  const size_t Cs = static_cast<size_t>(std::max<int64_t>(C, 1));
-  SR_TRY_CUDA(ctx, g.h_groups.ensure(std::max<size_t>(table.size(), 1)));
-  if (!table.empty()) std::memcpy(g.h_groups.p, table.data(), table.size() * sizeof(int32_t));
-  SR_TRY_CUDA(ctx, g.groups.ensure(std::max<size_t>(table.size(), 1)));
-  SR_TRY_CUDA(ctx, g.const_off.ensure(static_cast<size_t>(E) + 1));
-  SR_TRY_CUDA(ctx, g.const_cnt.ensure(static_cast<size_t>(std::max(E, 1))));
-  SR_TRY_CUDA(ctx, g.bwd_lo.ensure(static_cast<size_t>(std::max(E, 1))));
-  if (gtape_floats > 0) SR_TRY_CUDA(ctx, g.gtape.ensure(static_cast<size_t>(gtape_floats)));
-  SR_TRY_CUDA(ctx, g.const_loc.ensure(Cs));
-  SR_TRY_CUDA(ctx, g.grad_acc.ensure(Cs));
-  SR_TRY_CUDA(ctx, g.grad.ensure(Cs));
-  SR_TRY_CUDA(ctx, g.consts.ensure(Cs));
-  SR_TRY_CUDA(ctx, g.m.ensure(Cs));
-  SR_TRY_CUDA(ctx, g.v.ensure(Cs));
-  if (spill_floats > 0) SR_TRY_CUDA(ctx, ctx->spill.ensure(static_cast<size_t>(spill_floats)));
-  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
-                       std::max<int64_t>(static_cast<int64_t>(g.n_spans) * E, 1))));
-  SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
-  cudaStream_t s = ctx->stream;
-  if (!table.empty())
-    SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.groups.p, g.h_groups.p, table.size() * sizeof(int32_t),
-                                     cudaMemcpyHostToDevice, s));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.const_off.p, g.h_const_off.p, (E + 1) * sizeof(int64_t),
-                                   cudaMemcpyHostToDevice, s));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.const_cnt.p, g.h_const_cnt.p, E * sizeof(int32_t),
-                                   cudaMemcpyHostToDevice, s));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.bwd_lo.p, g.h_bwd_lo.p, E * sizeof(int32_t),
-                                   cudaMemcpyHostToDevice, s));
-  if (C > 0) {
-    SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.const_loc.p, g.h_const_loc.p, C * sizeof(int64_t),
-                                     cudaMemcpyHostToDevice, s));
-    SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.consts.p, g.h_consts.p, C * sizeof(float),
-                                     cudaMemcpyHostToDevice, s));
-  }
-  ctx->prep_stats.node_evals = ps.n_tokens * ctx->N;
-  ctx->prep_stats.node_evals_executed = ctx->prep_stats.node_evals;
-  return SR_OK;
-}
-
-// Forward + adjoint of every class, then mse / grad.
-sr_status launch_grad(sr_context *ctx) {
-  sr::GradSet &g = ctx->grad;
-  ProgramSet &ps = ctx->main;
-  cudaStream_t s = ctx->stream;
-  if (g.C > 0) SR_TRY_CUDA(ctx, cudaMemsetAsync(g.grad_acc.p, 0, g.C * sizeof(double), s));
-  SR_TRY_CUDA(ctx, record_event(ctx, 1));
-  for (const sr::AdjClass &cl : g.classes) {
-    if (cl.plan.items() == 0) continue;
-    sr::AdjArgs a{};
-    a.e = make_args(ctx, ps, ctx->d_counter);
-    a.e.W = cl.plan.W;
-    a.e.smax = cl.plan.smax;
-    a.e.s_smem = cl.plan.s_smem;
-    a.e.G = cl.plan.G;
-    a.e.n_groups = cl.plan.n_groups;
-    a.e.span = cl.plan.span;
-    a.e.n_spans = cl.plan.n_spans;
-    a.e.group_expr = g.groups.p + cl.group_off;
-    a.const_off = g.const_off.p;
-    a.const_cnt = g.const_cnt.p;
-    a.bwd_lo = g.bwd_lo.p;
-    a.grad_acc = g.grad_acc.p;
-    a.gtape = cl.global_tape ? g.gtape.p : nullptr;
-    a.tape_len = cl.tape_len;
-    a.seg_cap = cl.seg_cap;
-    a.gmax = cl.gmax;
-    SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
-    SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.blocks, cl.plan.smem, s));
-  }
-  SR_TRY_CUDA(ctx, record_event(ctx, 2));
-  SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E, g.const_off.p,
-                                            g.const_cnt.p, g.grad_acc.p, ctx->mse.p, g.grad.p, s));
-  return SR_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode, float *mse_out,
-                       float *grad_out, sr_stats *stats) {
-  SR_TRACE("sr_eval_grad");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  if (mode != SR_GRAD_CHECKPOINT && mode != SR_GRAD_RECOMPUTE)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "unknown gradient mode");
-  const double t0 = now_ms();
-  const uint32_t flags = SR_EVAL_GRADIENT | (mode == SR_GRAD_RECOMPUTE ? SR_EVAL_GRAD_RECOMPUTE : 0u);
-  SR_TRY(sr_prepare(ctx, pop, flags));
-  if (pop->num_exprs == 0) {
-    if (stats) *stats = sr_stats{};
-    return SR_OK;
-  }
-  SR_TRY(sr_launch(ctx));
-  SR_TRY(sr_read_mse(ctx, mse_out, nullptr));
-  if (grad_out) SR_TRY(sr_read_grad(ctx, grad_out));
-  if (stats) {
-    fill_stats(ctx, stats);
-    stats->total_eval_time_ms = now_ms() - t0;
-  }
-  return SR_OK;
-}
-
-sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
-                                const sr_adam_options *adam, float *const_out, float *mse_out,
-                                sr_stats *stats) {
-  SR_TRACE("sr_optimize_constants");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  if (!adam || adam->steps < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad Adam options");
-  if (adam->mode != SR_GRAD_CHECKPOINT && adam->mode != SR_GRAD_RECOMPUTE)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "unknown gradient mode");
-  SR_TRY(check_population(ctx, pop));
-  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
-  if (pop->num_exprs == 0) return SR_OK;
-  if (!mse_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "mse_out is NULL");
-  DeviceScope scope(ctx->device);
-  const double t0 = now_ms();
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  reset_prepared(ctx);
-  ctx->prep_stats = sr_stats{};
-  ctx->E = pop->num_exprs;
-  SR_TRY(prepare_grad(ctx, pop, adam->mode == SR_GRAD_RECOMPUTE));
-  ctx->mode = sr::Mode::kGrad;
-  sr::GradSet &g = ctx->grad;
-  cudaStream_t s = ctx->stream;
-  if (g.C > 0) {
-    SR_TRY_CUDA(ctx, cudaMemsetAsync(g.m.p, 0, g.C * sizeof(float), s));
-    SR_TRY_CUDA(ctx, cudaMemsetAsync(g.v.p, 0, g.C * sizeof(float), s));
-  }
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
-  int launches = 0;
-  for (int step = 1; step <= adam->steps; ++step) {
-    SR_TRY(launch_grad(ctx));
-    SR_TRY_CUDA(ctx, sr::launch_adam(g.C, g.grad.p, g.m.p, g.v.p, g.consts.p, g.const_loc.p,
-                                     ctx->main.code.p, step, adam->lr, adam->beta1, adam->beta2,
-                                     adam->eps, s));
-    launches += static_cast<int>(g.classes.size()) + 2;
-  }
-  SR_TRY(launch_grad(ctx));  // MSE at the final constants
-  launches += static_cast<int>(g.classes.size()) + 1;
-  SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[3], s));
-  ctx->timing_valid = true;
-  const int E = pop->num_exprs;
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_mse.p, ctx->mse.p, E * sizeof(float),
-                                   cudaMemcpyDeviceToHost, s));
-  if (g.C > 0 && const_out)
-    SR_TRY_CUDA(ctx, cudaMemcpyAsync(const_out, g.consts.p, g.C * sizeof(float),
-                                     cudaMemcpyDeviceToHost, s));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),
-                                   cudaMemcpyDeviceToHost, s));
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(s));
-  SR_TRY(check_device_error(ctx));
-  std::memcpy(mse_out, ctx->h_mse.p, E * sizeof(float));
-  ctx->prep_stats.kernel_launches = launches;
-  if (stats) {
-    fill_stats(ctx, stats);
-    stats->total_eval_time_ms = now_ms() - t0;
-  }
-  return SR_OK;
-}
-
-sr_status sr_eval_mse_fp64(sr_context *ctx, const sr_population *pop, double *mse64_out) {
-  SR_TRACE("sr_eval_mse_fp64");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  SR_TRY(check_population(ctx, pop));
-  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
-  const int E = pop->num_exprs;
-  if (E == 0) return SR_OK;
-  if (!mse64_out) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "mse64_out is NULL");
-  DeviceScope scope(ctx->device);
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  reset_prepared(ctx);
-  ctx->prep_stats = sr_stats{};
-  for (int x = 0; x < E; ++x) {  // the FP64 kernel's stack is shallower than the plain one's
-    int depth = 0, maxd = 0;
-    for (int64_t i = pop->offsets[x + 1] - 1; i >= pop->offsets[x]; --i) {
-      const int t = pop->tokens[i];
-      if (t <= 0) ++depth;
-      else if (sr::is_binary_token(t)) --depth;
-      maxd = std::max(maxd, depth);
-    }
-    if (maxd > sr::kFp64Stack)
-      return ctx->fail(SR_ERR_UNSUPPORTED, "expression " + std::to_string(x) +
-                                               " is deeper than the FP64 reference stack (" +
-                                               std::to_string(sr::kFp64Stack) + ")");
-  }
-  SR_TRY(prepare_plain(ctx, pop));  // raw tokens on the device, as the plain kernel reads them
-  SR_TRY_CUDA(ctx, ctx->mse64.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->h_mse64.ensure(static_cast<size_t>(E)));
-  sr::PlainSet &ps = ctx->plain;
-  SR_TRY_CUDA(ctx, sr::launch_fp64(ps.tok.p, ps.val.p, ps.off.p, ps.len.p, ctx->X.p, ctx->ldx,
-                                   ctx->V, ctx->N, E, ctx->partial.p, ps.n_dpblocks,
-                                   ctx->mse64.p, ctx->stream));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_mse64.p, ctx->mse64.p, E * sizeof(double),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  std::memcpy(mse64_out, ctx->h_mse64.p, E * sizeof(double));
-  return SR_OK;
-}
-
-// ---- the generation loop on the device ------------------------------------------
-
-sr_status sr_evolve_options_init(sr_evolve_options *o, int32_t num_vars) {
-  if (!o) return SR_ERR_INVALID_ARGUMENT;
-  *o = sr_evolve_options{};
-  // Reference EvolutionParams defaults (src/utils/utils.h:178-187) and loop
-  // constants (src/cleaned/cl_sr_system.cpp:293-309).
-  o->num_vars = num_vars;
-  o->max_tokens = 64;
-  o->max_depth = 5;
-  o->tournament = 3;
-  o->const_min = -5.0f;
-  o->const_max = 5.0f;
-  o->prob_leaf = 0.1f;
-  o->prob_const_leaf = 0.5f;
-  o->prob_unary = 0.35f;
-  o->elite_frac = 0.05f;
-  o->mutation_prob = 0.2f;
-  o->n_unary = 18;  // SIN .. LOOSE_SQRT (utils.cpp:939-943)
-  for (int k = 0; k < 18; ++k) o->unary_ops[k] = 10 + k;
-  o->n_binary = 9;  // ADD .. LOOSE_POW (utils.cpp:945-948)
-  for (int k = 0; k < 9; ++k) o->binary_ops[k] = 1 + k;
-  o->seed = 0x5EED5EEDull;
-  return SR_OK;
-}
-
-}  // extern "C"
-
-namespace {
-
-sr_status evolve_params(sr_context *ctx, const sr_evolve_options *o, int E, int stride,
-                        sr::EvolveParams *p) {
-  if (!o) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "evolve options are NULL");
-  if (E < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "negative population size");
-  if (o->num_vars < 0 || o->num_vars > SR_MAX_VARS)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "num_vars out of range");
-  if (o->max_tokens < 1 || o->max_depth < 0 || o->max_depth > 62 || o->tournament < 1)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad max_tokens / max_depth / tournament");
-  if (stride < o->max_tokens || stride > SR_EVOLVE_MAX_STRIDE)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT,
-                     "stride must lie in [max_tokens, " + std::to_string(SR_EVOLVE_MAX_STRIDE) +
-                         "]");
-  if (o->n_unary < 1 || o->n_unary > 32 || o->n_binary < 1 || o->n_binary > 16)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "operator tables must be non-empty");
-  for (int k = 0; k < o->n_unary; ++k)
-    if (!sr::is_unary_token(o->unary_ops[k]))
-      return ctx->fail(SR_ERR_BAD_TOKEN, "unary_ops[" + std::to_string(k) + "] is not unary");
-  for (int k = 0; k < o->n_binary; ++k)
-    if (!sr::is_binary_token(o->binary_ops[k]))
-      return ctx->fail(SR_ERR_BAD_TOKEN, "binary_ops[" + std::to_string(k) + "] is not binary");
-  const float probs[] = {o->prob_leaf, o->prob_const_leaf, o->prob_unary, o->elite_frac,
-                         o->mutation_prob};
-  for (float q : probs)
-    if (!(q >= 0.0f && q <= 1.0f)) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "probability outside [0, 1]");
-  if (!(o->const_min <= o->const_max)) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "const_min > const_max");
-  sr::EvolveParams q{};
-  q.num_vars = o->num_vars;
-  q.max_tokens = o->max_tokens;
-  q.max_depth = o->max_depth;
-  q.tournament = o->tournament;
-  q.const_min = o->const_min;
-  q.const_max = o->const_max;
-  q.prob_leaf = o->prob_leaf;
-  q.prob_const_leaf = o->prob_const_leaf;
-  q.prob_unary = o->prob_unary;
-  q.mutation_prob = o->mutation_prob;
-  q.n_unary = o->n_unary;
-  q.n_binary = o->n_binary;
-  std::memcpy(q.unary_ops, o->unary_ops, sizeof q.unary_ops);
-  std::memcpy(q.binary_ops, o->binary_ops, sizeof q.binary_ops);
-  q.seed = o->seed;
-  *p = q;
-  return SR_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-sr_status sr_evolve_init(sr_context *ctx, const sr_evolve_options *opts, int32_t num_exprs,
-                         int32_t stride, int32_t *tokens, float *values, int32_t *lengths) {
-  SR_TRACE("sr_evolve_init");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  sr::EvolveParams p;
-  SR_TRY(evolve_params(ctx, opts, num_exprs, stride, &p));
-  if (num_exprs == 0) return SR_OK;
-  if (!tokens || !values || !lengths) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL buffer");
-  DeviceScope scope(ctx->device);
-  SR_TRY_CUDA(ctx, sr::launch_evolve_init(p, num_exprs, stride, tokens, values, lengths,
-                                          ctx->stream));
-  return SR_OK;
-}
-
-sr_status sr_evolve_step(sr_context *ctx, const sr_evolve_options *opts, int32_t generation,
-                         int32_t num_exprs, int32_t stride, const float *fitness,
-                         const int32_t *tokens, const float *values, const int32_t *lengths,
-                         int32_t *tokens_out, float *values_out, int32_t *lengths_out) {
-  SR_TRACE("sr_evolve_step");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  sr::EvolveParams p;
-  SR_TRY(evolve_params(ctx, opts, num_exprs, stride, &p));
-  const int E = num_exprs;
-  if (E == 0) return SR_OK;
-  if (!fitness || !tokens || !values || !lengths || !tokens_out || !values_out || !lengths_out)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL buffer");
-  const size_t slots = static_cast<size_t>(E) * static_cast<size_t>(stride);
-  auto overlaps = [&](const void *a, const void *b, size_t bytes) {
-    const char *x = static_cast<const char *>(a), *y = static_cast<const char *>(b);
-    return x < y + bytes && y < x + bytes;
-  };
-  if (overlaps(tokens, tokens_out, slots * sizeof(int32_t)) ||
-      overlaps(values, values_out, slots * sizeof(float)) ||
-      overlaps(lengths, lengths_out, static_cast<size_t>(E) * sizeof(int32_t)))
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "output buffers overlap the inputs");
-  DeviceScope scope(ctx->device);
-  const size_t temp = sr::rank_temp_bytes(E);
-  const bool grow = ctx->evo_temp.cap < std::max<size_t>(temp, 1) ||
-                    ctx->evo_keys.cap < 2 * static_cast<size_t>(E) ||
-                    ctx->evo_order.cap < static_cast<size_t>(E);
-  if (grow) SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  SR_TRY_CUDA(ctx, ctx->evo_temp.ensure(std::max<size_t>(temp, 1)));
-  SR_TRY_CUDA(ctx, ctx->evo_keys.ensure(2 * static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->evo_idx.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->evo_order.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->evo_fit.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, sr::launch_rank(fitness, E, ctx->evo_temp.p, ctx->evo_temp.cap,
-                                   ctx->evo_keys.p, ctx->evo_idx.p, ctx->evo_order.p,
-                                   ctx->evo_fit.p, ctx->stream));
-  int elites = static_cast<int>(static_cast<double>(E) * static_cast<double>(opts->elite_frac));
-  elites = std::min(std::max(elites, 1), E);
-  SR_TRY_CUDA(ctx, sr::launch_evolve_step(p, generation, E, stride, elites, ctx->evo_order.p,
-                                          ctx->evo_fit.p, tokens, values, lengths, tokens_out,
-                                          values_out, lengths_out, ctx->stream));
-  return SR_OK;
-}
-
-sr_status sr_prepare_device_population(sr_context *ctx, const int32_t *tokens,
-                                       const float *values, const int32_t *lengths,
-                                       int32_t num_exprs, int32_t stride) {
-  SR_TRACE("sr_prepare_device_population");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  if (num_exprs < 0 || stride < 1 || stride > SR_EVOLVE_MAX_STRIDE)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad population size or stride");
-  if (num_exprs > 0 && (!tokens || !values || !lengths))
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL buffer");
-  if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
-  DeviceScope scope(ctx->device);
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  reset_prepared(ctx);
-  ctx->prep_stats = sr_stats{};
-  const int E = num_exprs;
-  ctx->E = E;
-  if (E == 0) return SR_OK;
-  const double t0 = now_ms();
-  ProgramSet &ps = ctx->main;
-  ps.E = E;
-  const size_t n_code = static_cast<size_t>(E) * (static_cast<size_t>(stride) + 1) + 1;
-  SR_TRY_CUDA(ctx, ps.code.ensure(n_code));
-  SR_TRY_CUDA(ctx, ps.off.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ps.len.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->evo_summary.ensure(8));
-  SR_TRY_CUDA(ctx, ctx->h_evo_summary.ensure(8));
-  SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
-  // The interpreter prefetches one instruction past a program: keep the
-  // padding word defined.
-  SR_TRY_CUDA(ctx, cudaMemsetAsync(ps.code.p + (n_code - 1), 0, sizeof(Instr), ctx->stream));
-  SR_TRY_CUDA(ctx, sr::launch_compile_device(tokens, values, lengths, E, stride, ctx->V,
-                                             ps.code.p, ps.off.p, ps.len.p, ctx->evo_summary.p,
-                                             ctx->stream));
-  SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_evo_summary.p, ctx->evo_summary.p, 8 * sizeof(int32_t),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  const int32_t *sm = ctx->h_evo_summary.p;
-  if (sm[1] != 0)
-    return ctx->fail(SR_ERR_MALFORMED_EXPRESSION,
-                     "the device population holds an invalid expression (or one longer than "
-                     "the stride)");
-  int64_t n_tok = 0, n_ins = 0;
-  std::memcpy(&n_tok, sm + 2, sizeof n_tok);
-  std::memcpy(&n_ins, sm + 4, sizeof n_ins);
-  ps.smax = sm[0];
-  ps.n_tokens = n_tok;
-  ps.n_instr = n_ins;
-  ps.n_instr_protected = sm[6];
-  ps.cache_refs = false;  // compiled without cache hints
-  ps.cost.assign(static_cast<size_t>(E), 0.0f);  // groups in population order
-  ps.n_const.assign(static_cast<size_t>(E), 0);
-  ps.sfu_per_dp = 0.0;
-  ps.fp32_per_dp = 0.0;
-  ctx->prep_stats.host_compile_time_ms = now_ms() - t0;
-  // No timing here: a generation loop would re-tune whenever its populations
-  // move to another shape class; the tuned shape of a class is used when the
-  // context has one, else the profile's default.
-  SR_TRY(prepare_main_shape(ctx, false));
-  ctx->prep_stats.node_evals = n_tok * ctx->N;
-  ctx->prep_stats.node_evals_executed = ctx->prep_stats.node_evals;
-  ctx->mode = sr::Mode::kBatched;
-  return SR_OK;
-}
-
-sr_status sr_get_stream(sr_context *ctx, void **stream) {
-  if (!ctx || !stream) return SR_ERR_INVALID_ARGUMENT;
-  *stream = ctx->stream;
-  return SR_OK;
-}
-
-sr_status sr_synchronize(sr_context *ctx) {
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  DeviceScope scope(ctx->device);
-  SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return SR_OK;
-}
-
-sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s, double *sfu_ops_per_s,
-                           int32_t *num_sms) {
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  DeviceScope scope(ctx->device);
-  float *dummy = nullptr;
-  SR_TRY_CUDA(ctx, cudaMalloc(&dummy, 1024 * sizeof(float)));
-  const int blocks = ctx->num_sms * 8, threads = 256, iters = 8192;
-  double rates[2] = {0, 0};
-  for (int m = 0; m < 2; ++m) {
-    const bool mufu = (m == 1);
-    float best = 1e30f;
-    for (int rep = 0; rep < 4; ++rep) {
-      cudaEventRecord(ctx->ev[4], ctx->stream);
-      const cudaError_t e = sr::launch_pipe_bench(mufu, dummy, blocks, threads, iters, ctx->stream);
-      cudaEventRecord(ctx->ev[5], ctx->stream);
-      if (e != cudaSuccess || cudaEventSynchronize(ctx->ev[5]) != cudaSuccess) {
-        cudaFree(dummy);
-        return cuda_fail(ctx, e != cudaSuccess ? e : cudaGetLastError(), "pipe benchmark");
-      }
-      const float ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
-      if (rep > 0) best = std::min(best, ms);
-    }
-    rates[m] = static_cast<double>(blocks) * threads * iters * 8.0 / (best * 1e-3);
-  }
-  cudaFree(dummy);
-  if (fp32_ops_per_s) *fp32_ops_per_s = rates[0];
-  if (sfu_ops_per_s) *sfu_ops_per_s = rates[1];
-  if (num_sms) *num_sms = ctx->num_sms;
-  return SR_OK;
-}
-
-sr_status sr_measure_operator_rates(sr_context *ctx, const int32_t *ops, int32_t n_ops,
-                                   double *evals_per_s) {
-  SR_TRACE("sr_measure_operator_rates");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  if (n_ops < 0 || (n_ops > 0 && (!ops || !evals_per_s)))
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad operator list");
-  for (int32_t i = 0; i < n_ops; ++i)
-    if (!(ops[i] >= 0 && ops[i] <= 27) && ops[i] != static_cast<int32_t>(sr::kOpExpClamp))
-      return ctx->fail(SR_ERR_BAD_TOKEN, "operator " + std::to_string(ops[i]) + " has no rate kernel");
-  DeviceScope scope(ctx->device);
-  float *dummy = nullptr;
-  SR_TRY_CUDA(ctx, cudaMalloc(&dummy, 1024 * sizeof(float)));
-  const int blocks = ctx->num_sms * 8, threads = 256, iters = 256;
-  for (int32_t i = 0; i < n_ops; ++i) {
-    float best = 1e30f;
-    for (int rep = 0; rep < 4; ++rep) {
-      cudaEventRecord(ctx->ev[4], ctx->stream);
-      const cudaError_t e = sr::launch_op_rate(ops[i], dummy, blocks, threads, iters, ctx->stream);
-      cudaEventRecord(ctx->ev[5], ctx->stream);
-      if (e != cudaSuccess || cudaEventSynchronize(ctx->ev[5]) != cudaSuccess) {
-        cudaFree(dummy);
-        return cuda_fail(ctx, e != cudaSuccess ? e : cudaGetLastError(), "operator rate");
-      }
-      const float ms = elapsed_ms(ctx->ev[4], ctx->ev[5]);
-      if (rep > 0) best = std::min(best, ms);
-    }
-    evals_per_s[i] = static_cast<double>(blocks) * threads * iters * 8.0 / (best * 1e-3);
-  }
-  cudaFree(dummy);
-  return SR_OK;
-}
-
-}  // extern "C"
-
-// ---- host-only helpers ------------------------------------------------------
-extern "C" {
-
-uint64_t sr_subtree_key(const int32_t *tokens, const double *values, int32_t len) {
-  if (!tokens || !values || len <= 0) return sr::kFnvOffset;
-  return sr::flat_key(tokens, values, len);
-}
-
-sr_status sr_subtree_hashes(const int32_t *tokens, const double *values, int32_t len,
-                            int32_t *sizes, uint64_t *hashes) {
-  if (!tokens || !values || !sizes || !hashes || len < 0) return SR_ERR_INVALID_ARGUMENT;
-  sr::merkle_hashes(tokens, values, len, sizes, hashes);
-  return SR_OK;
-}
-
-sr_status sr_detect_subtrees(const sr_population *pop, int32_t min_size, int32_t min_freq,
-                             int32_t max_groups, sr_detect_result *res, int32_t *group_expr,
-                             int32_t *group_pos, int32_t *group_size, int32_t *group_count,
-                             uint64_t *group_key) {
-  SR_TRACE("sr_detect_subtrees");
-  if (!pop || !res || pop->num_exprs < 0 || min_size < 1 || min_freq < 1)
-    return SR_ERR_INVALID_ARGUMENT;
-  if (pop->num_exprs > 0 && (!pop->tokens || !pop->values || !pop->offsets))
-    return SR_ERR_INVALID_ARGUMENT;
-  sr::Detection det;
-  sr::detect_common_subtrees(pop->num_exprs, pop->tokens, pop->values, pop->offsets, min_size,
-                             min_freq, static_cast<int>(std::thread::hardware_concurrency()), det);
-  res->num_subtrees = static_cast<int32_t>(det.groups.size());
-  res->total_tokens = det.total_tokens;
-  res->covered_tokens = det.covered_tokens;
-  res->avg_subtree_size = det.avg_subtree_size;
-  res->coverage = det.coverage;
-  const int n = std::min<int>(std::max(max_groups, 0), static_cast<int>(det.groups.size()));
-  for (int g = 0; g < n; ++g) {
-    const auto &G = det.groups[static_cast<size_t>(g)];
-    if (group_expr) group_expr[g] = G.expr;
-    if (group_pos) group_pos[g] = G.pos;
-    if (group_size) group_size[g] = G.size;
-    if (group_count) group_count[g] = G.occurrences;
-    if (group_key)
-      group_key[g] = sr::flat_key(pop->tokens + pop->offsets[G.expr] + G.pos,
-                                  pop->values + pop->offsets[G.expr] + G.pos, G.size);
-  }
-  return SR_OK;
-}
-
-sr_status sr_detect_subtrees_device(sr_context *ctx, const sr_population *pop, int32_t min_size,
-                                    int32_t min_freq, int32_t max_groups, sr_detect_result *res,
-                                    int32_t *group_expr, int32_t *group_pos, int32_t *group_size,
-                                    int32_t *group_count, uint64_t *group_key) {
-  SR_TRACE("sr_detect_subtrees_device");
-  if (!ctx) return SR_ERR_INVALID_ARGUMENT;
-  ctx->last_error.clear();
-  if (!pop || !res || pop->num_exprs < 0 || min_size < 1 || min_freq < 1)
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad detection arguments");
-  if (pop->num_exprs > 0 && (!pop->tokens || !pop->values || !pop->offsets))
-    return ctx->fail(SR_ERR_INVALID_ARGUMENT, "NULL population arrays");
-  DeviceScope scope(ctx->device);
-  sr::Detection det;
-  SR_TRY(detect_on_device(ctx, pop->num_exprs, pop->tokens, pop->values, pop->offsets, min_size,
-                          min_freq, det));
-  res->num_subtrees = static_cast<int32_t>(det.groups.size());
-  res->total_tokens = det.total_tokens;
-  res->covered_tokens = det.covered_tokens;
-  res->avg_subtree_size = det.avg_subtree_size;
-  res->coverage = det.coverage;
-  const int n = std::min<int>(std::max(max_groups, 0), static_cast<int>(det.groups.size()));
-  for (int g = 0; g < n; ++g) {
-    const auto &G = det.groups[static_cast<size_t>(g)];
-    if (group_expr) group_expr[g] = G.expr;
-    if (group_pos) group_pos[g] = G.pos;
-    if (group_size) group_size[g] = G.size;
-    if (group_count) group_count[g] = G.occurrences;
-    if (group_key)
-      group_key[g] = sr::flat_key(pop->tokens + pop->offsets[G.expr] + G.pos,
-                                  pop->values + pop->offsets[G.expr] + G.pos, G.size);
-  }
-  return SR_OK;
-}
-
-sr_status sr_mark_cached(const sr_population *pop, const uint64_t *keys, const int32_t *slots,
-                         int32_t n_keys, int32_t *hints) {
-  if (!pop || pop->num_exprs < 0 || n_keys < 0 || (n_keys > 0 && (!keys || !slots)))
-    return SR_ERR_INVALID_ARGUMENT;
-  if (pop->num_exprs == 0) return SR_OK;
-  if (!pop->tokens || !pop->values || !pop->offsets || !hints) return SR_ERR_INVALID_ARGUMENT;
-  sr::SubtreeCache cache;
-  cache.capacity = n_keys;
-  for (int32_t k = 0; k < n_keys; ++k) cache.slot_of.emplace(keys[k], slots[k]);
-  cache.used = n_keys;
-  sr::mark_cached_subtrees(pop->num_exprs, pop->tokens, pop->values, pop->offsets, cache,
-                           static_cast<int>(std::thread::hardware_concurrency()), hints);
-  return SR_OK;
-}
-
-sr_status sr_validate_population(const sr_population *pop, int32_t num_vars, int32_t *n_instr,
-                                 int32_t *spill_slots, int32_t *bad_expr) {
-  if (bad_expr) *bad_expr = -1;
-  if (!pop || pop->num_exprs < 0 || num_vars < 0) return SR_ERR_INVALID_ARGUMENT;
-  if (pop->num_exprs == 0) return SR_OK;
-  if (!pop->tokens || !pop->values || !pop->offsets || pop->offsets[0] != 0)
-    return SR_ERR_INVALID_ARGUMENT;
-  std::vector<sr::Instr> scratch;
-  for (int x = 0; x < pop->num_exprs; ++x) {
-    const int64_t o = pop->offsets[x];
-    const int64_t len = pop->offsets[x + 1] - o;
-    sr::ExprInfo info;
-    sr_status s;
-    if (len <= 0) {
-      s = SR_ERR_MALFORMED_EXPRESSION;
-    } else if (len > SR_MAX_TOKENS) {
-      s = SR_ERR_EXPRESSION_TOO_LONG;
-    } else {
-      scratch.clear();
-      s = sr::compile_expression(pop->tokens + o, pop->values + o, static_cast<int>(len),
-                                 num_vars, nullptr, scratch, info, nullptr);
-    }
-    if (s != SR_OK) {
-      if (bad_expr) *bad_expr = x;
-      return s;
-    }
-    if (n_instr) n_instr[x] = info.n_instr;
-    if (spill_slots) spill_slots[x] = info.need;
-  }
-  return SR_OK;
-}
-
-}  // extern "C"
-
-extern "C" sr_status sr_compile_population(const sr_population *pop, int32_t num_vars,
-                                           uint32_t *code, int64_t code_capacity,
-                                           int64_t *instr_offsets, int32_t *spill_slots) {
-  if (!pop || pop->num_exprs < 0 || num_vars < 0 || !instr_offsets || code_capacity < 0)
-    return SR_ERR_INVALID_ARGUMENT;
-  instr_offsets[0] = 0;
-  if (pop->num_exprs == 0) return SR_OK;
-  if (!pop->tokens || !pop->values || !pop->offsets || pop->offsets[0] != 0)
-    return SR_ERR_INVALID_ARGUMENT;
-  std::vector<sr::Instr> out;
-  for (int x = 0; x < pop->num_exprs; ++x) {
-    const int64_t o = pop->offsets[x];
-    const int64_t len = pop->offsets[x + 1] - o;
-    if (len <= 0) return SR_ERR_MALFORMED_EXPRESSION;
-    if (len > SR_MAX_TOKENS) return SR_ERR_EXPRESSION_TOO_LONG;
-    sr::ExprInfo info;
-    const sr_status s = sr::compile_expression(pop->tokens + o, pop->values + o,
-                                               static_cast<int>(len), num_vars, nullptr, out,
-                                               info, nullptr);
-    if (s != SR_OK) return s;
-    instr_offsets[x + 1] = static_cast<int64_t>(out.size());
-    if (spill_slots) spill_slots[x] = info.need;
-  }
-  if (code) {
-    if (static_cast<int64_t>(out.size()) > code_capacity) return SR_ERR_INVALID_ARGUMENT;
-    std::memcpy(code, out.data(), out.size() * sizeof(sr::Instr));
-  }
-  return SR_OK;
-}
