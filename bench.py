@@ -58,6 +58,10 @@ def parse_args():
                     help="also time the plain per-expression kernel")
     ap.add_argument("--exprs", type=int, default=0,
                     help="population size override (profiling cases)")
+    ap.add_argument("--dps", type=int, default=0,
+                    help="with --profile-launch: datapoint count override")
+    ap.add_argument("--cached", action="store_true",
+                    help="with --profile-launch: evaluate through the subtree cache")
     ap.add_argument("--dpt", type=int, default=0, help="force datapoints per thread")
     ap.add_argument("--warps", type=int, default=0, help="force evaluating warps per block")
     ap.add_argument("--profile-launch", action="store_true",
@@ -72,22 +76,24 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", "1")))
 
 
-def make_workload(name: str, rank: int, exprs: int = 0):
+def make_workload(name: str, rank: int, exprs: int = 0, dps: int = 0):
     from symbolic_regression_gpu_b200 import synth
     fn = synth.WORKLOADS[name]
     seeds = {"plain": 1, "batched": 2, "cache": 3, "grad": 4, "large": 5}
     kw = {"E": exprs} if exprs > 0 else {}
+    if dps > 0:
+        kw["N"] = dps
     return fn(seed=seeds[name] + 1000 * rank, **kw)
 
 
 def profile_launch(args):
     """One prepared evaluation on GPU 0, nothing timed (the ncu capture case)."""
     from symbolic_regression_gpu_b200 import Evaluator, _lib
-    w = make_workload(args.workload, 0, args.exprs)
+    w = make_workload(args.workload, 0, args.exprs, args.dps)
     with Evaluator(device=0, dpt=args.dpt, warps_per_block=args.warps) as ev:
         ev.set_data(w.X)
         if args.grad_mode == "none":
-            ev.prepare(w.population)
+            ev.prepare(w.population, cache=args.cached, clear_cache=args.cached)
         else:
             mode = (_lib.SR_GRAD_CHECKPOINT if args.grad_mode == "checkpoint"
                     else _lib.SR_GRAD_RECOMPUTE)
