@@ -170,6 +170,9 @@ sr_status compile_set(sr_context *ctx, int E, const int32_t *tok, const double *
 
 // Operator profile of a compiled set (the evaluation launches; prediction
 // launches always use kOpsAll).
+// Shortest datapoint span the planner shrinks to for occupancy.
+constexpr int64_t kMinSpan = 256;
+
 bool protected_profile(const ProgramSet &ps) {
   return ps.n_instr > 0 &&
          static_cast<double>(ps.n_instr_protected) >= sr::kProtectedShare * ps.n_instr;
@@ -201,6 +204,27 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
          sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, static_cast<int>(span)) >
              static_cast<size_t>(dev_max_smem))
     span = std::max<int64_t>(tile, (span / 2) / tile * tile);
+  // Then, while the span's shared memory (the X buffers grow with the
+  // variable count) rather than the registers limits the resident blocks,
+  // halve it: more resident warps pay for more, shorter work items
+  // (9 variables, 8 datapoints x 8 warps: 2 -> 3 blocks per SM at 512).
+  if (span_target > 0) {
+    int bps_now = 0;
+    SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache,
+                                          sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem,
+                                                                static_cast<int>(span)),
+                                          W, &bps_now));
+    while (span / 2 >= std::max<int64_t>(tile, kMinSpan) && (span / 2) % tile == 0) {
+      int bps_half = 0;
+      SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache,
+                                            sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem,
+                                                                  static_cast<int>(span / 2)),
+                                            W, &bps_half));
+      if (bps_half <= bps_now) break;
+      span /= 2;
+      bps_now = bps_half;
+    }
+  }
   // The kernel walks a span tile by tile: it must hold whole tiles.
   if (span % tile != 0) return ctx->fail(SR_ERR_UNSUPPORTED, "span is not a multiple of the tile");
   p.span = static_cast<int>(span);
