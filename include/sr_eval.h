@@ -370,13 +370,20 @@ sr_status sr_compile_population(const sr_population *pop, int32_t num_vars, uint
  * the work; its partial sums live in one fixed array built into the
  * library (SR_NOALLOC_SCRATCH_BYTES, resident on every GPU that loads the
  * library until exit), so no call allocates.  The first call on a device
- * looks up that array's device address (one-time set-up; make that first
- * call before any stream capture).  The call runs on `stream` (NULL = the
- * default stream) and waits for it before returning.  Calls share the
- * array: calls whose kernels overlap on the GPU race and their results are
- * undefined.  Expressions are validated on the device: a malformed one gets
- * a NaN MSE and the call returns SR_ERR_MALFORMED_EXPRESSION.  num_exprs >
- * SR_NOALLOC_MAX_EXPRS returns SR_ERR_UNSUPPORTED. */
+ * looks up that array's device address (one-time set-up, repeated only if
+ * the device's context was reset in between; make that first call before
+ * any stream capture).  The call runs on `stream` (NULL = the default
+ * stream) and waits for it before returning.  Calls share the array: calls
+ * whose kernels overlap on the GPU race and their results are undefined.
+ * offsets: off[0] >= 0 and off[num_exprs] must be the length of the tokens
+ * and values buffers (the kernel reads only tokens in [off[0],
+ * off[num_exprs]) and checks every expression's offsets against those two).
+ * Expressions are validated on the device before they are evaluated, also
+ * when num_dps is 0: one whose offsets are inconsistent, with no token or
+ * more than SR_MAX_TOKENS, an unknown token, or a stack that underflows or
+ * does not end with exactly one value gets a NaN MSE and the call returns
+ * SR_ERR_MALFORMED_EXPRESSION.  num_exprs > SR_NOALLOC_MAX_EXPRS returns
+ * SR_ERR_UNSUPPORTED. */
 #define SR_NOALLOC_SCRATCH_BYTES (4u << 20)
 #define SR_NOALLOC_MAX_EXPRS ((int32_t)((SR_NOALLOC_SCRATCH_BYTES - 256u) / 16u))
 sr_status sr_eval_mse_device_noalloc(const int32_t *tokens, const float *values,

@@ -13,39 +13,10 @@
 #include <cstdint>
 #include <cstdlib>
 #include <string>
+#include <thread>
 #include <vector>
 
-namespace {
-struct PackedInfo {
-  InputInfo info{};
-  std::vector<int> nv, nd, nt;
-  std::vector<int *> tp;
-  std::vector<double *> vp;
-  PackedInfo(int E, const int *tok, const double *val, const long long *off, int V, int N) {
-    nv.assign(E, V);
-    nd.assign(E, N);
-    nt.resize(E);
-    tp.resize(E);
-    vp.resize(E);
-    for (int i = 0; i < E; ++i) {
-      nt[i] = static_cast<int>(off[i + 1] - off[i]);
-      tp[i] = const_cast<int *>(tok + off[i]);
-      vp[i] = const_cast<double *>(val + off[i]);
-    }
-    info.num_exprs = E;
-    info.num_vars = nv.data();
-    info.num_dps = nd.data();
-    info.num_tokens = nt.data();
-    info.tokens = tp.data();
-    info.values = vp.data();
-    info.data_filenames = nullptr;
-    info.tokens_packed = nullptr;
-    info.values_packed_f32 = nullptr;
-    info.X_packed_f32 = nullptr;
-    info.has_shared_data = true;
-  }
-};
-}  // namespace
+#include "ref_pack.hpp"
 
 extern "C" {
 
@@ -57,16 +28,37 @@ float ref_eval_single(const int *tok, const double *val, int n, const float *var
 // evaluate_cpu_mse (cl_cpu_eval.cpp:94-168) over a column-major dataset.
 double ref_eval_mse(int E, const int *tok, const double *val, const long long *off, int V, int N,
                     const float *X, float *mse_out, int threads) {
-  PackedInfo p(E, tok, val, off, V, N);
-  std::vector<float *> rows(V + 1);
-  for (int v = 0; v <= V; ++v) rows[v] = const_cast<float *>(X) + static_cast<size_t>(v) * N;
-  std::vector<float **> all(E, rows.data());
+  refpack::PackedInfo p(E, tok, val, off, V, N, X);
   setenv("THREADS", std::to_string(threads).c_str(), 1);
   std::vector<float> mses;
   RunStats st;
-  evaluate_cpu_mse(p.info, all.data(), mses, st);
+  evaluate_cpu_mse(p.info, p.all.data(), mses, st);
   for (int i = 0; i < E; ++i) mse_out[i] = mses[i];
   return st.total_eval_time_ms;
+}
+
+// evaluate_single_expr at every datapoint, out[e * N + dp], on `threads`
+// threads over contiguous expression ranges.
+void ref_predict_all(int E, const int *tok, const double *val, const long long *off, int V,
+                     int N, const float *X, float *out, int threads) {
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> th;
+  for (int k = 0; k < threads; ++k) {
+    th.emplace_back([=]() {
+      std::vector<float> dpv(V > 0 ? V : 1);
+      const int e0 = static_cast<int>(static_cast<long long>(E) * k / threads);
+      const int e1 = static_cast<int>(static_cast<long long>(E) * (k + 1) / threads);
+      for (int e = e0; e < e1; ++e) {
+        const int n = static_cast<int>(off[e + 1] - off[e]);
+        for (int dp = 0; dp < N; ++dp) {
+          for (int v = 0; v < V; ++v) dpv[v] = X[static_cast<size_t>(v) * N + dp];
+          out[static_cast<size_t>(e) * N + dp] =
+              evaluate_single_expr(tok + off[e], val + off[e], n, dpv.data(), V);
+        }
+      }
+    });
+  }
+  for (auto &t : th) t.join();
 }
 
 // compute_hash (detect.cpp:50-68)

@@ -45,29 +45,97 @@ static __device__ __align__(256) unsigned char noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-void *g_scratch_addr[kMaxDevices] = {};  // device address of noalloc_scratch, per device
+// Per device: the device address of noalloc_scratch and the id of the CUDA
+// context it belongs to.  A device reset (cudaDeviceReset) makes a new
+// context in which the array has a new address, so the address is looked up
+// again whenever the current context is not the one it was looked up in.
+void *g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
 
-// One-time set-up per device, with that device current: the host-side name
-// of a __device__ array is only a stand-in, the kernel needs its device
-// address.
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (the
+// library does not link the driver library itself).
+typedef int (*ctx_get_current_fn)(void **ctx);
+typedef int (*ctx_get_id_fn)(void *ctx, unsigned long long *id);
+
+bool current_context_id(unsigned long long *id) {
+  static ctx_get_current_fn get_current = nullptr;
+  static ctx_get_id_fn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) !=
+            cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || !f1)
+      return false;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) !=
+            cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f2)
+      return false;
+    get_current = reinterpret_cast<ctx_get_current_fn>(f1);
+    get_id = reinterpret_cast<ctx_get_id_fn>(f2);
+  }
+  void *ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx) return false;
+  return get_id(ctx, id) == 0;
+}
+
+// Set-up per device (and per context of that device), with that device
+// current: the host-side name of a __device__ array is only a stand-in, the
+// kernel needs its device address.  Called by every call (under a mutex);
+// it looks the address up only on the first call in a context.
 sr_status scratch_address(int device, unsigned char **out) {
   if (device < 0 || device >= kMaxDevices) return SR_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[device]) {
+  unsigned long long ctx_id = 0;
+  if (!current_context_id(&ctx_id)) return SR_ERR_CUDA;
+  if (!g_scratch_addr[device] || g_scratch_ctx[device] != ctx_id) {
     void *ptr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&ptr, noalloc_scratch);
     if (e != cudaSuccess || !ptr) return SR_ERR_CUDA;
     g_scratch_addr[device] = ptr;
+    g_scratch_ctx[device] = ctx_id;
   }
   *out = static_cast<unsigned char *>(g_scratch_addr[device]);
   return SR_OK;
 }
 
+// Structural check of expression e, made before anything of it is read for
+// evaluation: its offsets lie in [off[0], off[E]] (off[0] >= 0, and the
+// caller's contract is that off[E] is the length of the token and value
+// buffers), it has 1..SR_MAX_TOKENS tokens, every token is known, the
+// right-to-left evaluation never pops an empty stack or holds more than
+// kPlainStack values, and exactly one value is left at the end.
+__device__ bool expr_well_formed(const int32_t *__restrict__ tok,
+                                 const int64_t *__restrict__ off, int e, int E) {
+  const int64_t lo = off[0], hi = off[E];
+  const int64_t o = off[e], o1 = off[e + 1];
+  if (!(lo >= 0 && lo <= o && o <= o1 && o1 <= hi)) return false;
+  const int64_t len = o1 - o;
+  if (len < 1 || len > SR_MAX_TOKENS) return false;
+  int sp = 0;
+  for (int64_t i = len - 1; i >= 0; --i) {
+    const int t = tok[o + i];
+    if (t == SR_TOK_CONST || t == SR_TOK_VAR) {
+      if (++sp > kPlainStack) return false;
+    } else if (t >= 1 && t <= 9) {
+      if (sp < 2) return false;
+      --sp;
+    } else if ((t >= 10 && t <= 27) || t == SR_OP_EXP_CLAMP) {
+      if (sp < 1) return false;
+    } else {
+      return false;
+    }
+  }
+  return sp == 1;
+}
+
 // Plain-kernel variant over device-resident tokens: 4 expressions x 128
 // datapoints per block, token stack in local memory, squared errors reduced
-// in FP64 per block into partial[blockIdx.y][e].  Malformed expressions
-// (unknown token, stack underflow / overflow, not exactly one result) set
-// error bit 1 and contribute no valid datapoint.
+// in FP64 per block into partial[blockIdx.y][e].  Every block first checks
+// the structure of its 4 expressions (expr_well_formed); a malformed one is
+// never evaluated, contributes no valid datapoint (NaN MSE) and, in the
+// blocks of row blockIdx.y == 0, sets error bit 1.  The grid has at least
+// one row, so the check also runs when there are no datapoints.
 __global__ void __launch_bounds__(128)
     plain_checked_kernel(const int32_t *__restrict__ tok, const float *__restrict__ val,
                          const int64_t *__restrict__ off, const float *__restrict__ X,
@@ -75,7 +143,15 @@ __global__ void __launch_bounds__(128)
                          int32_t *__restrict__ error) {
   __shared__ double red_s[4][4];
   __shared__ int red_c[4][4];
+  __shared__ bool well_formed[4];
   const int e0 = blockIdx.x * 4;
+  if (threadIdx.x < 4) {
+    const int e = e0 + static_cast<int>(threadIdx.x);
+    const bool ok = e < E && expr_well_formed(tok, off, e, E);
+    well_formed[threadIdx.x] = ok;
+    if (e < E && !ok && blockIdx.y == 0) atomicOr(error, 1);
+  }
+  __syncthreads();
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   int cnt[4] = {0, 0, 0, 0};
   for (int64_t dp = static_cast<int64_t>(blockIdx.y) * 128 + threadIdx.x; dp < N;
@@ -85,41 +161,29 @@ __global__ void __launch_bounds__(128)
     const float yv = xc[V];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
+      if (!well_formed[j]) continue;  // also every e >= E
       const int e = e0 + j;
-      if (e >= E) break;
       const int64_t o = off[e];
       const int64_t len = off[e + 1] - o;
+      // Well-formed: the stack stays within [1, kPlainStack] and one value
+      // is left at the end.
       float stk[kPlainStack];
       int sp = 0;
-      bool ok = len >= 1 && len <= SR_MAX_TOKENS;
-      for (int64_t i = len - 1; ok && i >= 0; --i) {
+      for (int64_t i = len - 1; i >= 0; --i) {
         const int t = tok[o + i];
         if (t == SR_TOK_CONST) {
-          ok = sp < kPlainStack;
-          if (ok) stk[sp++] = val[o + i];
+          stk[sp++] = val[o + i];
         } else if (t == SR_TOK_VAR) {
-          ok = sp < kPlainStack;
           const float fv = val[o + i];
           const int vi = (fv > -2147483648.0f && fv < 2147483648.0f) ? static_cast<int>(fv) : -1;
-          if (ok) stk[sp++] = (vi >= 0 && vi < V) ? xc[vi] : 0.0f;
+          stk[sp++] = (vi >= 0 && vi < V) ? xc[vi] : 0.0f;
         } else if (t >= 1 && t <= 9) {
-          ok = sp >= 2;
-          if (ok) {
-            const float v1 = stk[--sp];
-            const float v2 = stk[--sp];
-            stk[sp++] = op_binary(t, v1, v2);
-          }
-        } else if ((t >= 10 && t <= 27) || t == SR_OP_EXP_CLAMP) {
-          ok = sp >= 1;
-          if (ok) stk[sp - 1] = op_unary(t, stk[sp - 1]);
+          const float v1 = stk[--sp];
+          const float v2 = stk[--sp];
+          stk[sp++] = op_binary(t, v1, v2);
         } else {
-          ok = false;
+          stk[sp - 1] = op_unary(t, stk[sp - 1]);
         }
-      }
-      ok = ok && sp == 1;
-      if (!ok) {
-        if (threadIdx.x == 0 && blockIdx.y == 0) atomicOr(error, 1);
-        continue;
       }
       const float pred = stk[0];
       if (isfinite(pred)) {
@@ -179,21 +243,22 @@ extern "C" sr_status sr_eval_mse_device_noalloc(const int32_t *tokens, const flo
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   // Datapoint blocks: up to 256, fewer when the partial sums of all
-  // expressions would not fit the fixed scratch.
+  // expressions would not fit the fixed scratch (E <= capacity keeps at
+  // least one), and at least one, so that the structural check of the
+  // expressions also runs when there are no datapoints.
   int64_t dpblocks = (num_dps + 127) / 128;
   dpblocks = dpblocks < 256 ? dpblocks : 256;
   const int64_t fit = static_cast<int64_t>(sr::kPartialCapacity) / num_exprs;
   if (dpblocks > fit) dpblocks = fit;
+  if (dpblocks < 1) dpblocks = 1;
 
   // The error word must start at zero; the partial sums are fully
   // overwritten by every launch that reads them.
   if (cudaMemsetAsync(d_error, 0, sizeof(int32_t), s) != cudaSuccess) return SR_ERR_CUDA;
-  if (dpblocks > 0) {
-    const dim3 grid(static_cast<unsigned>((num_exprs + 3) / 4), static_cast<unsigned>(dpblocks));
-    sr::plain_checked_kernel<<<grid, 128, 0, s>>>(tokens, values, offsets, X, ld, num_vars,
-                                                   num_dps, num_exprs, partial, d_error);
-    if (cudaGetLastError() != cudaSuccess) return SR_ERR_CUDA;
-  }
+  const dim3 grid(static_cast<unsigned>((num_exprs + 3) / 4), static_cast<unsigned>(dpblocks));
+  sr::plain_checked_kernel<<<grid, 128, 0, s>>>(tokens, values, offsets, X, ld, num_vars,
+                                                 num_dps, num_exprs, partial, d_error);
+  if (cudaGetLastError() != cudaSuccess) return SR_ERR_CUDA;
   if (sr::launch_finalize(partial, static_cast<int>(dpblocks), num_exprs, mse_out, s) !=
       cudaSuccess)
     return SR_ERR_CUDA;

@@ -3,11 +3,13 @@
 Runs the reference's CPU evaluator (evaluate_single_expr / evaluate_cpu_mse,
 src/cleaned/cl_cpu_eval.cpp), its subtree hashing and detection
 (src/utils/detect.cpp) and its cache marking (src/cleaned/cl_gpu_eval.cu:294-329),
-all compiled unchanged into oracle/_ref/libref_oracle.so by `make -C oracle ref`,
-on seeded inputs, and stores inputs and outputs as .npz files.  The fixtures
-are committed; the tests never need the reference tree.
+all compiled unchanged into oracle/_ref/libref_oracle.so, and the same CPU
+evaluator with the one added case for opcode 32 (exp clamped at 80,
+oracle/_ref/libref_expc.so, see oracle/ref_expc_shim.cpp), on seeded inputs,
+and stores inputs and outputs as .npz files.  The fixtures are committed; the
+tests never need the reference tree.
 
-    python tests/golden/make_golden.py
+    make -C oracle REF=<reference tree> ref && python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -121,6 +123,66 @@ def eval_workload_fixture():
           X=X, mse=mse, pred_E=np.int64(40), pred_N=np.int64(300), pred=pred)
 
 
+def _exp_clamp_dataset(rng, V: int, N: int) -> np.ndarray:
+    """Arguments around the clamp (80), the float overflow of exp (88.72...)
+    and beyond (100, 1e30, inf), NaN, and large negative ones."""
+    X = rng.uniform(-3, 3, size=(V + 1, N)).astype(np.float32)
+    around = np.array([79.0, 79.99999, 80.0, 80.00001, 80.5, 81.0, 88.0, 88.7, 88.72, 88.7228,
+                       88.73, 89.0, 100.0, 1e30, np.inf, np.nan, -80.0, -87.3, -103.9, -104.0,
+                       -120.0, -np.inf, 0.0, -0.0, 1e-40, 40.0, 44.35, 45.0], np.float32)
+    k = min(N, around.size)
+    for v in range(V):
+        X[v, 3 * v:3 * v + k] = np.roll(around, 5 * v)[:k]
+    X[V] = rng.uniform(-2, 2, N).astype(np.float32)
+    return X
+
+
+def _exp_clamp_expressions():
+    C, X, EC = op.TOK_CONST, op.TOK_VAR, op.EXP_CLAMP
+    return [
+        ([EC, X], [0.0, 0.0]),
+        ([EC, X], [0.0, 1.0]),
+        ([EC, op.MUL, C, X], [0.0, 0.0, 30.0, 2.0]),          # 30 x: arguments up to +-90
+        ([EC, op.NEG, X], [0.0, 0.0, 0.0]),
+        ([EC, EC, X], [0.0, 0.0, 0.0]),                       # clamp of a clamped exp
+        ([op.ADD, EC, X, EC, X], [0.0, 0.0, 0.0, 0.0, 1.0]),   # 2 e^80 stays finite
+        ([op.MUL, EC, X, EC, X], [0.0, 0.0, 0.0, 0.0, 1.0]),   # e^160 overflows
+        ([op.SUB, EC, X, EC, X], [0.0, 0.0, 0.0, 0.0, 0.0]),
+        ([op.LOOSE_LOG, EC, X], [0.0, 0.0, 0.0]),
+        ([op.LOOSE_DIV, C, EC, X], [0.0, 1.0, 0.0, 1.0]),
+        ([EC, op.LOOSE_DIV, X, C], [0.0, 0.0, 0.0, 0.0125]),  # x / 0.0125: 80 at x = 1
+        ([EC, C], [0.0, 80.0]),
+        ([EC, C], [0.0, 88.7228]),
+        ([EC, C], [0.0, 100.0]),
+        ([op.EXP, X], [0.0, 0.0]),                            # the unclamped reference EXP
+    ]
+
+
+def eval_exp_clamp_fixture():
+    """Opcode 32 at arguments around 80, 88.7 and 100 (edge expressions) and
+    the workload operators with opcode 32 itself (random expressions), from
+    the reference evaluator with the added case."""
+    rng = np.random.default_rng(501)
+    V, N = 3, 300
+    X = _exp_clamp_dataset(rng, V, N)
+    edge = Population.from_lists(_exp_clamp_expressions())
+    pred = oracle.refx_predict(edge, X)
+    mse, _ = oracle.refx_mse(edge, X, threads=4)
+    rng = np.random.default_rng(502)
+    V2, N2 = 5, 1000
+    X2 = rng.uniform(-3, 3, size=(V2 + 1, N2)).astype(np.float32)
+    X2[0, :40] = rng.uniform(20, 95, 40).astype(np.float32)   # large exp arguments
+    pop = synth.small_random_population(503, 200, V2, max_len=63, binary=op.WORKLOAD_BINARY,
+                                        unary=op.WORKLOAD_UNARY)
+    mse2, _ = oracle.refx_mse(pop, X2, threads=4)
+    sub = pop.slice(0, 60)
+    pred2 = oracle.refx_predict(sub, X2[:, :400].copy())
+    _save("eval_exp_clamp.npz", tokens=edge.tokens, values=edge.values, offsets=edge.offsets,
+          X=X, pred=pred, mse=mse, w_tokens=pop.tokens, w_values=pop.values,
+          w_offsets=pop.offsets, w_X=X2, w_mse=mse2, w_pred_E=np.int64(60),
+          w_pred_N=np.int64(400), w_pred=pred2)
+
+
 def hash_fixture():
     pop = _population_all_ops(301, 60, 4, 50)
     keys_ref, keys_gpu_path, sizes_ref, merkle_ref = [], [], [], []
@@ -159,10 +221,17 @@ def detect_fixture():
 
 
 def main():
-    if not oracle.reference_available():
-        sys.exit("oracle/_ref/libref_oracle.so is missing: run `make -C oracle ref` first")
+    if not (oracle.reference_available() and oracle.reference_expc_available()):
+        sys.exit("oracle/_ref/libref_oracle.so or libref_expc.so is missing: run "
+                 "`make -C oracle REF=<reference tree> ref` first")
+    only = set(sys.argv[1:])
+    if only:
+        for name in only:
+            globals()[name]()
+        return
     eval_fixture()
     eval_workload_fixture()
+    eval_exp_clamp_fixture()
     hash_fixture()
     detect_fixture()
 

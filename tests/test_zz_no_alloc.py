@@ -34,9 +34,13 @@ def _device_population(torch, pop: Population):
     return tok, val, off
 
 
-def _noalloc(torch, pop: Population, X: np.ndarray):
+def _noalloc(torch, pop: Population, X: np.ndarray, offsets=None):
+    """One call through the C ABI; offsets (int64, num_exprs + 1) replaces the
+    population's own to plant inconsistent ones."""
     dev = torch.device("cuda", 0)
     tok, val, off = _device_population(torch, pop)
+    if offsets is not None:
+        off = torch.from_numpy(np.asarray(offsets, np.int64)).to(dev)
     Xd = torch.from_numpy(np.ascontiguousarray(X, np.float32)).to(dev)
     out = torch.full((pop.num_exprs,), -1.0, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -88,3 +92,73 @@ def test_noalloc_rejects_malformed_and_oversized():
     # A well-formed call right after still works.
     st, mse = _noalloc(torch, w.population, w.X)
     assert st == _lib.SR_OK
+
+
+def test_noalloc_rejects_inconsistent_offsets_and_checks_without_datapoints():
+    torch = pytest.importorskip("torch")
+    torch.cuda.init()
+    w = synth.plain_workload(seed=64, E=6, N=2000)
+    pop = w.population
+    good = pop.offsets.copy()
+    # Offsets that step backwards or past off[E] are rejected for their
+    # expression only; every other expression is still evaluated.
+    back = good.copy()
+    back[2] = back[3] + 1          # expression 1 runs into 3, expression 2 ends before it starts
+    st, mse = _noalloc(torch, pop, w.X, offsets=back)
+    assert st == _lib.SR_ERR_MALFORMED_EXPRESSION
+    assert np.isnan(mse[1]) and np.isnan(mse[2])
+    with sg.Evaluator(device=0) as ev:
+        ev.set_data(w.X)
+        ref = ev.eval_mse(pop)
+    keep = [0, 3, 4, 5]
+    _check_against_regular(mse[keep], ref[keep])
+    beyond = good.copy()
+    beyond[-2] = beyond[-1] + 5    # the last two expressions would end / start past off[E]
+    st, mse = _noalloc(torch, pop, w.X, offsets=beyond)
+    assert st == _lib.SR_ERR_MALFORMED_EXPRESSION
+    assert np.isnan(mse[-1]) and np.isnan(mse[-2])
+    # With no datapoints the structure is still checked: a malformed
+    # expression is reported, and every MSE is NaN (no valid datapoint).
+    X0 = np.zeros((w.X.shape[0], 0), np.float32)
+    bad = Population.from_lists(list(pop) + [([op.SIN], [0.0])])
+    st, mse = _noalloc(torch, bad, X0)
+    assert st == _lib.SR_ERR_MALFORMED_EXPRESSION
+    assert np.isnan(mse).all()
+    st, mse = _noalloc(torch, pop, X0)
+    assert st == _lib.SR_OK
+    assert np.isnan(mse).all()
+
+
+def test_noalloc_large_population_fewer_datapoint_blocks():
+    """5,000 expressions x 40,000 datapoints: the partial sums of 256 datapoint
+    blocks would not fit the fixed array, so the call runs fewer blocks (52),
+    each covering more datapoints; the results match the regular entry point."""
+    torch = pytest.importorskip("torch")
+    torch.cuda.init()
+    w = synth.batched_workload(seed=65, E=5000, N=40_000, generations=1)
+    assert (_lib.SR_NOALLOC_SCRATCH_BYTES - 256) // 16 // 5000 < (40_000 + 127) // 128
+    with sg.Evaluator(device=0) as ev:
+        ev.set_data(w.X)
+        ref = ev.eval_mse(w.population)
+    for _ in range(2):
+        st, mse = _noalloc(torch, w.population, w.X)
+        assert st == _lib.SR_OK, _lib.status_string(st)
+        _check_against_regular(mse, ref)
+
+
+def test_noalloc_maximum_population():
+    """SR_NOALLOC_MAX_EXPRS expressions (one datapoint block each) on a small
+    dataset: the largest population the fixed array holds."""
+    torch = pytest.importorskip("torch")
+    torch.cuda.init()
+    base = synth.plain_workload(seed=66, E=48, N=300)
+    reps = -(-_lib.SR_NOALLOC_MAX_EXPRS // base.population.num_exprs)
+    from symbolic_regression_gpu_b200.population import concat
+    pop = concat([base.population] * reps).slice(0, _lib.SR_NOALLOC_MAX_EXPRS)
+    with sg.Evaluator(device=0) as ev:
+        ev.set_data(base.X)
+        ref = ev.eval_mse(base.population)
+    st, mse = _noalloc(torch, pop, base.X)
+    assert st == _lib.SR_OK, _lib.status_string(st)
+    want = np.resize(ref, pop.num_exprs)
+    _check_against_regular(mse, want)
