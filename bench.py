@@ -8,10 +8,13 @@ an original expression evaluated at one datapoint.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun, one rank per GPU; every rank evaluates its own
-seeded shard of the population (weak scaling, no collective on the data path).
-`--impl reference` times the reference's own CPU evaluator (evaluate_cpu_mse,
-compiled unchanged into oracle/_ref) on the host cores instead.
+N > 1 runs one rank per GPU (when not started by torchrun, bench.py starts
+torchrun itself); every rank evaluates its own seeded shard of the population
+(weak scaling, no collective on the data path; the end-to-end step ends with
+the MSE all-gather).  `--impl reference` times the reference's own CPU
+evaluator (evaluate_cpu_mse, compiled unchanged into oracle/_ref) on the host
+cores instead.  `--check-launch` runs the multi-rank plumbing alone (any
+backend, no GPU needed) and prints the ranks it formed.
 """
 from __future__ import annotations
 
@@ -52,10 +55,19 @@ def parse_args():
                     help="skip the subtree-cache figures")
     ap.add_argument("--no-evolution", action="store_true",
                     help="skip the device generation-loop figures")
-    ap.add_argument("--large", action="store_true",
-                    help="also run the 100,000 x 4M population (about two minutes)")
-    ap.add_argument("--plain-baseline", action="store_true",
-                    help="also time the plain per-expression kernel")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 100,000 x 4M population (forward, fused forward+adjoint, "
+                         "plain kernel; about a minute)")
+    ap.add_argument("--no-plain-baseline", action="store_true",
+                    help="skip the plain per-expression kernel on the headline population")
+    ap.add_argument("--no-plain-config", action="store_true",
+                    help="skip the plain-forward workload at full size (1,000 x 100k)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's own GPU evaluators on the headline population")
+    ap.add_argument("--check-launch", action="store_true",
+                    help="form the ranks, build each rank's shard, all-gather a per-expression "
+                         "vector, print the ranks (no GPU work; gloo works)")
+    ap.add_argument("--backend", default="nccl", help="process-group backend of --check-launch")
     ap.add_argument("--exprs", type=int, default=0,
                     help="population size override (profiling cases)")
     ap.add_argument("--dps", type=int, default=0,
@@ -84,6 +96,52 @@ def make_workload(name: str, rank: int, exprs: int = 0, dps: int = 0):
     if dps > 0:
         kw["N"] = dps
     return fn(seed=seeds[name] + 1000 * rank, **kw)
+
+
+def relaunch_under_torchrun(args) -> int:
+    """--gpus N > 1 without a torchrun environment: start N ranks of this same
+    command under torchrun (one process per GPU, rendezvous on 127.0.0.1) and
+    return its exit status.  Rank 0 prints the JSON line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1",
+           f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def check_launch(args) -> int:
+    """The multi-rank plumbing of the bench without GPU work: every rank
+    builds its own seeded shard (as the measured run does), the ranks
+    all-gather one float per expression (the MSE all-gather of the end-to-end
+    step, here the expressions' token counts) and rank 0 checks the gathered
+    vector against the shards it rebuilds itself and prints the ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from symbolic_regression_gpu_b200 import sharding
+    rank, local_rank, world = dist_env()
+    dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=60))
+    dev = torch.device("cuda", local_rank) if args.backend == "nccl" else torch.device("cpu")
+    w = make_workload(args.workload, rank, args.exprs, args.dps)
+    local = np.diff(w.population.offsets).astype(np.float32)
+    E = w.population.num_exprs
+    bounds = np.arange(world + 1, dtype=np.int64) * E
+    got = sharding.gather_mse(local, bounds, device=dev)
+    if rank == 0:
+        want = np.concatenate([np.diff(make_workload(args.workload, r, args.exprs,
+                                                     args.dps).population.offsets)
+                               for r in range(world)]).astype(np.float32)
+        print(json.dumps({"n_gpus": world, "backend": args.backend, "exprs_per_rank": E,
+                          "gathered": int(got.size),
+                          "gathered_ok": bool(np.array_equal(got, want))}))
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
 
 
 def profile_launch(args):
@@ -194,32 +252,73 @@ def _ulp_distance(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return np.where(na & nb, 0, np.where(na | nb, 1 << 40, d))
 
 
-def parity_figures(ev, w, sample, ours_mse, ref_mse):
-    """Parity of the GPU path against the reference on the CPU-baseline sample:
-    MSE against the reference's evaluate_cpu_mse, per-datapoint ulp against the
-    reference's per-datapoint evaluation (the oracle's predict_f32, pinned bit
-    for bit to evaluate_single_expr) on sampled datapoints, and the reduction
-    error alone (our MSE against an FP64 sum of our own FP32 predictions)."""
+def _import_generators_only():
+    """Make the package's pure-Python workload generators (synth, population,
+    opcodes) importable without running the package __init__, which loads
+    libsr_eval.so: the reference arm must not map the product library."""
+    import types
+    if "symbolic_regression_gpu_b200" in sys.modules:
+        return
+    pkg = types.ModuleType("symbolic_regression_gpu_b200")
+    pkg.__path__ = [os.path.join(ROOT, "symbolic_regression_gpu_b200")]
+    sys.modules["symbolic_regression_gpu_b200"] = pkg
+
+
+def _rule_summary(r: dict) -> dict:
+    n = max(int(r.get("expressions", r.get("datapoints", 0))), 1)
+    out = dict(r)
+    out["exempt_flagged_frac"] = r["exempt_flagged"] / n
+    out["exempt_conditioning_frac"] = r["exempt_conditioning"] / n
+    return out
+
+
+def parity_figures(ev, w, sample, ours_mse, ref_mse, threads, patched):
+    """Parity of the GPU path against the reference on the CPU-baseline sample
+    (outside the timed region), under the condition-aware rule (oracle
+    error_bound / mse_parity / datapoint_parity):
+      * MSE against the reference's evaluate_cpu_mse on the whole sample (raw
+        agreement), and the rule on its first 96 expressions over all
+        datapoints;
+      * per datapoint against the reference's evaluate_single_expr on 512
+        expressions x 4,096 datapoints;
+      * the reduction error alone (our MSE against an FP64 sum of our own FP32
+        predictions);
+      * accuracy against the FP64 evaluation under the rule's mode 1 on the
+        same 96 expressions."""
     from oracle import oracle
-    out = {}
+    out = {"reference": ("evaluate_cpu_mse / evaluate_single_expr with the one added "
+                         "exp-clamp case (oracle/_ref/libref_expc.so)") if patched else
+           "the oracle's restatement of evaluate_cpu_mse (pinned bit for bit by the goldens)"}
     with np.errstate(invalid="ignore", divide="ignore"):
         r = np.abs(np.asarray(ours_mse, np.float64) - ref_mse) / np.maximum(np.abs(ref_mse), 1e-300)
     both = np.isfinite(ours_mse) & np.isfinite(ref_mse)
     out["mse_vs_reference_cpu"] = {
-        "expressions": int(both.sum()),
+        "expressions": int(sample.num_exprs), "finite": int(both.sum()),
         "median_rel": float(np.median(r[both])) if both.any() else None,
         "frac_le_1e-6": float(np.mean(r[both] <= 1e-6)) if both.any() else None,
-        "nan_pattern_equal": bool(np.array_equal(np.isnan(ours_mse), np.isnan(ref_mse)))}
+        "nan_pattern_equal": bool(np.array_equal(np.isnan(ours_mse), np.isnan(ref_mse))),
+        "inf_pattern_equal": bool(np.array_equal(np.isinf(ours_mse), np.isinf(ref_mse)))}
+    k = min(96, sample.num_exprs)
+    sub = sample.slice(0, k)
+    b = oracle.error_bound(sub, w.X, mode=0, threads=threads)
+    out["mse_rule"] = _rule_summary(oracle.mse_parity(ours_mse[:k], ref_mse[:k],
+                                                      b["mse_bound"], b["flagged"]))
+    out["mse_rule"]["datapoints"] = int(w.num_dps)
     ns = min(4096, w.num_dps)
-    sub = sample.subset(np.arange(min(512, sample.num_exprs)))
-    ours = ev.predictions(sub, 0, ns)
-    theirs = oracle.predict_f32(sub, np.ascontiguousarray(w.X[:, :ns]))
+    sub2 = sample.slice(0, min(512, sample.num_exprs))
+    Xs = np.ascontiguousarray(w.X[:, :ns])
+    ours = ev.predictions(sub2, 0, ns)
+    theirs = oracle.refx_predict(sub2, Xs, threads) if patched else oracle.predict_f32(sub2, Xs)
+    bb = oracle.error_bound(sub2, Xs, mode=0, per_datapoint=True, threads=threads)
+    rd = oracle.datapoint_parity(ours, theirs, bb["bound"], bb["flag"])
     u = _ulp_distance(ours, theirs)
-    out["per_datapoint_ulp"] = {
-        "expressions": int(sub.num_exprs), "datapoints": int(ns),
-        "bit_identical": float(np.mean(u == 0)), "frac_le_4ulp": float(np.mean(u <= 4)),
-        "violations_gt_4ulp": int(np.count_nonzero(u > 4))}
-    red = sample.subset(np.arange(min(16, sample.num_exprs)))
+    rd = _rule_summary(rd)
+    rd.update({"expressions": int(sub2.num_exprs), "datapoints_per_expression": int(ns),
+               "bit_identical_frac": float(np.mean(u == 0)),
+               "frac_le_4ulp": float(np.mean(u <= 4)),
+               "raw_gt_4ulp": int(np.count_nonzero(u > 4))})
+    out["per_datapoint"] = rd
+    red = sample.slice(0, min(16, sample.num_exprs))
     pred = ev.predictions(red)
     sums = oracle.mse_of_predictions(pred, w.X[w.num_vars])
     del pred
@@ -229,14 +328,24 @@ def parity_figures(ev, w, sample, ours_mse, ref_mse):
     rr = rr[np.isfinite(rr)]
     out["reduction_error"] = {"expressions": int(red.num_exprs),
                               "max_rel": float(rr.max()) if rr.size else None}
+    m64 = ev.eval_mse_fp64(sub)
+    b1 = oracle.error_bound(sub, w.X, mode=1, threads=threads)
+    out["accuracy_rule_vs_fp64"] = _rule_summary(
+        oracle.mse_parity(ours_mse[:k], m64, b1["mse_bound"], b1["flagged"],
+                          bar=oracle.FP64_BAR))
     return out
 
 
 def cpu_baseline(w, target_s: float, threads: int):
-    """Reference evaluate_cpu_mse (oracle/_ref, compiled -O3) on a seeded
-    expression subset over the full datapoint range."""
+    """The reference CPU evaluator (oracle/_ref, compiled -O3) on a seeded
+    expression subset over the full datapoint range: its evaluate_cpu_mse
+    with the one added exp-clamp case when that build exists (so that the
+    same run's MSEs serve as the parity reference), else the unchanged build
+    with the exp-clamp opcode timed as its EXP (same expf call)."""
     from oracle import oracle
-    pop = _reference_population(w.population)
+    patched = oracle.reference_expc_available()
+    pop = w.population if patched else _reference_population(w.population)
+    fn = oracle.refx_mse if patched else oracle.ref_mse
     E = pop.num_exprs
     rng = np.random.default_rng(7)
     order = rng.permutation(E)
@@ -244,23 +353,98 @@ def cpu_baseline(w, target_s: float, threads: int):
     n_probe = max(threads, min(E, 16))
     probe = pop.subset(order[:n_probe])
     t0 = time.perf_counter()
-    oracle.ref_mse(probe, w.X, threads=threads)
+    fn(probe, w.X, threads=threads)
     rate = probe.num_tokens * w.num_dps / max(time.perf_counter() - t0, 1e-6)
     tokens_target = rate * target_s / w.num_dps
     mean_len = pop.num_tokens / E
     n = int(max(threads, min(E, tokens_target / mean_len)))
     sample = pop.subset(order[:n])
     t0 = time.perf_counter()
-    ref = oracle.ref_mse(sample, w.X, threads=threads)
+    ref = fn(sample, w.X, threads=threads)
     dt = time.perf_counter() - t0
     value = sample.num_tokens * w.num_dps / dt
-    ref_mse = np.asarray(ref[0] if isinstance(ref, tuple) else ref, np.float32)
+    ref_mse = np.asarray(ref[0], np.float32)
+    what = ("reference evaluate_cpu_mse (src/cleaned/cl_cpu_eval.cpp) with the one added "
+            "exp-clamp case" if patched else
+            "reference evaluate_cpu_mse (src/cleaned/cl_cpu_eval.cpp) unchanged, exp_clamp80 "
+            "timed as the reference EXP opcode")
     return {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-            "_sample_index": order[:n], "_sample_mse": ref_mse,
+            "_sample_index": order[:n], "_sample_mse": ref_mse, "_patched": patched,
             "sample": f"{n} of {E} expressions (seeded subset) x all {w.num_dps} datapoints, "
-                      f"{dt:.1f} s; reference evaluate_cpu_mse (src/cleaned/cl_cpu_eval.cpp) "
-                      f"compiled -O3, THREADS={threads}; exp_clamp80 timed as the reference "
-                      f"EXP opcode"}
+                      f"{dt:.1f} s; {what}, compiled -O3, THREADS={threads}"}
+
+
+def plain_config_figures(ev, torch, flush_buf, sr_stream, threads):
+    """The plain-forward workload at full size (1,000 ramped half-and-half
+    expressions, 3 variables, 100,000 datapoints): forward and plain-kernel
+    node-evals/s, and every MSE against the reference's under the rule (the
+    reference evaluator with the exp-clamp case, all 1,000 x 100,000, about a
+    second on the host cores)."""
+    from oracle import oracle
+    w = make_workload("plain", 0)
+    pop = w.population
+    node_evals = pop.num_tokens * w.num_dps
+    ev.set_data(w.X)
+    res = {"workload": "plain", "exprs": pop.num_exprs, "num_dps": w.num_dps,
+           "num_vars": w.num_vars}
+    for name, kw in (("fwd", {}), ("plain_kernel", {"plain": True})):
+        ev.prepare(pop, **kw)
+        _timed_launches(ev, torch, flush_buf, sr_stream, 2)
+        ms = statistics.mean(_timed_launches(ev, torch, flush_buf, sr_stream, 5))
+        res[name] = {"value": node_evals / (ms * 1e-3), "unit": UNIT, "ms": ms}
+    res["fwd"]["vs_plain_kernel"] = res["plain_kernel"]["ms"] / res["fwd"]["ms"]
+    ev.prepare(pop)
+    ev.launch()
+    mse = ev.read_mse()
+    patched = oracle.reference_expc_available()
+    t0 = time.perf_counter()
+    ref = (oracle.refx_mse(pop, w.X, threads)[0] if patched else
+           oracle.mse_f32(pop, w.X, threads))
+    cpu_s = time.perf_counter() - t0
+    b = oracle.error_bound(pop, w.X, mode=0, threads=threads)
+    r = _rule_summary(oracle.mse_parity(mse, ref, b["mse_bound"], b["flagged"]))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rel = np.abs(mse.astype(np.float64) - ref) / np.maximum(np.abs(ref), 1e-300)
+    fin = np.isfinite(rel)
+    r.update({"reference": "evaluate_cpu_mse with the exp-clamp case" if patched else
+              "restatement", "reference_cpu_s": cpu_s, "reference_cpu_threads": threads,
+              "median_rel": float(np.median(rel[fin])) if fin.any() else None,
+              "frac_le_1e-6": float(np.mean(rel[fin] <= 1e-6)) if fin.any() else None})
+    res["parity_full"] = r
+    return res
+
+
+def reference_gpu_figures(w, steps: int = 2):
+    """The reference's own GPU evaluators (plain and subtree-cache paths,
+    compiled unchanged for sm_100a) on the same population and dataset, in
+    their own process (oracle/ref_gpu.py: the reference prints to stdout and
+    exits on CUDA errors), chunked within their int32 index limits."""
+    import tempfile
+    from oracle import ref_gpu
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so was not built"}
+    why = ref_gpu.check_limits(w.population.tokens.copy(), w.population.values,
+                               w.population.offsets, w.num_vars, w.num_dps)
+    if why:
+        return {"unavailable": why}
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "pop.npz"), os.path.join(td, "res.json")
+        np.savez(inp, tokens=w.population.tokens, values=w.population.values,
+                 offsets=w.population.offsets, X=w.X)
+        t0 = time.perf_counter()
+        rc = subprocess.call([sys.executable, "-m", "oracle.ref_gpu", inp, out,
+                              "--steps", str(steps)], cwd=ROOT, timeout=900,
+                             stdout=subprocess.DEVNULL)
+        wall = time.perf_counter() - t0
+        if rc != 0 or not os.path.exists(out):
+            return {"unavailable": f"the reference GPU process exited with status {rc}"}
+        res = json.load(open(out))
+    res["process_wall_s"] = wall
+    res["what"] = ("evaluate_gpu_simple_wrapper and evaluate_gpu_mse_wrapper (src/cleaned/"
+                   "cl_gpu_simple.cu, cl_gpu_eval.cu) compiled unchanged for sm_100a, "
+                   "expression chunks with E_chunk x N < 2^31, exp_clamp80 run as EXP; "
+                   "kernel_* from the reference's own CUDA events, call_* its wall clock")
+    return res
 
 
 # ---- reference arm ------------------------------------------------------------------
@@ -269,6 +453,7 @@ def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return 0
+    _import_generators_only()
     from oracle import oracle
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference",
@@ -478,11 +663,14 @@ def large_figures(ev, rank, flush_buf, sr_stream):
     ev.set_data(w.X)
     res = {"workload": "large", "exprs": pop.num_exprs, "num_dps": w.num_dps,
            "num_vars": w.num_vars, "tokens": int(pop.num_tokens)}
-    for name, kw in (("fwd", {}),
-                     ("fwd_adjoint", {"gradient": True, "grad_mode": _lib.SR_GRAD_CHECKPOINT}),
-                     ("plain_kernel", {"plain": True})):
+    # The forward pass after one warm-up launch; the fused forward+adjoint and
+    # the plain kernel (seconds each) one launch after their prepare.
+    for name, kw, n in (("fwd", {}, 2),
+                        ("fwd_adjoint", {"gradient": True,
+                                         "grad_mode": _lib.SR_GRAD_CHECKPOINT}, 1),
+                        ("plain_kernel", {"plain": True}, 1)):
         ev.prepare(pop, **kw)
-        ms = _timed_launches(ev, torch, flush_buf, sr_stream, 2)[-1]
+        ms = _timed_launches(ev, torch, flush_buf, sr_stream, n)[-1]
         res[name] = {"value": node_evals / (ms * 1e-3), "unit": UNIT, "ms": ms}
     res["fwd_adjoint"]["cost_vs_fwd"] = res["fwd_adjoint"]["ms"] / res["fwd"]["ms"]
     res["fwd"]["vs_plain_kernel"] = res["plain_kernel"]["ms"] / res["fwd"]["ms"]
@@ -592,7 +780,7 @@ def run_ours(args):
 
     # Plain per-expression kernel on the same population (baseline ratio).
     plain = None
-    if args.plain_baseline and rank == 0:
+    if not args.no_plain_baseline and rank == 0:
         ev.prepare(w.population, plain=True)
         ev.launch()
         ev.read_mse()
@@ -601,7 +789,8 @@ def run_ours(args):
             a, _ = step()
             pm.append(a)
         plain = {"value": node_evals / (statistics.mean(pm) * 1e-3), "unit": UNIT,
-                 "ms_per_step": statistics.mean(pm)}
+                 "ms_per_step": statistics.mean(pm),
+                 "fwd_vs_plain_kernel": statistics.mean(pm) / (total_ms / len(step_ms))}
         ev.prepare(w.population)
 
     # Forward + adjoint on the constant-optimisation workload (4,096
@@ -617,8 +806,13 @@ def run_ours(args):
     if not args.no_evolution:
         evolution = evolution_figures(ev, w, torch, sr_stream)
     large = None
-    if args.large:
+    if not args.no_large:
         large = large_figures(ev, rank, flush_buf, sr_stream)
+        ev.set_data(w.X)
+    plain_config = None
+    if not args.no_plain_config and rank == 0 and world == 1:
+        plain_config = plain_config_figures(ev, torch, flush_buf, sr_stream,
+                                            os.cpu_count() or 1)
         ev.set_data(w.X)
 
     # End to end through the public API: pinned host dataset and host
@@ -673,7 +867,22 @@ def run_ours(args):
                         "finite": int(r.size)}
             cpu["accuracy_vs_fp64"] = {"reference_cpu": _stats(ref_mse),
                                        "this_gpu_same_expressions": _stats(mse[idx])}
-            cpu["parity"] = parity_figures(ev, w, sample, mse[idx], ref_mse)
+            cpu["parity"] = parity_figures(ev, w, sample, mse[idx], ref_mse,
+                                           os.cpu_count() or 1, cpu.pop("_patched"))
+
+    reference_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ev.synchronize()
+        try:
+            reference_gpu = reference_gpu_figures(w)
+        except (ImportError, OSError, subprocess.SubprocessError) as ex:
+            reference_gpu = {"unavailable": str(ex)}
+        if "kernel_node_evals_per_s" in reference_gpu.get("simple", {}):
+            reference_gpu["ours_fwd_vs_simple_kernel"] = (
+                value / reference_gpu["simple"]["kernel_node_evals_per_s"])
+        if "kernel_node_evals_per_s" in reference_gpu.get("subtree", {}):
+            reference_gpu["ours_fwd_vs_subtree_kernels"] = (
+                value / reference_gpu["subtree"]["kernel_node_evals_per_s"])
 
     if rank == 0:
         line = {
@@ -712,6 +921,8 @@ def run_ours(args):
             "subtree_cache": cache,
             "device_evolution": evolution,
             "large": large,
+            "plain_config": plain_config,
+            "reference_gpu": reference_gpu,
             "mse_finite": int(np.isfinite(mse).sum()),
             "accuracy_vs_fp64": accuracy,
         }
@@ -724,6 +935,10 @@ def run_ours(args):
 
 def main():
     args = parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch_under_torchrun(args)
+    if args.check_launch:
+        return check_launch(args)
     if args.profile_launch:
         return profile_launch(args)
     if args.impl == "reference":

@@ -11,8 +11,6 @@ from typing import Iterable, List, Sequence, Tuple
 
 import numpy as np
 
-from . import _lib
-
 
 @dataclass
 class Population:
@@ -75,8 +73,12 @@ class Population:
         return Population(self.tokens[a:b].copy(), self.values[a:b].copy(),
                           self.offsets[begin:end + 1] - a)
 
-    def as_c(self) -> _lib.sr_population:
-        """sr_population view; the Population must outlive its use."""
+    def as_c(self):
+        """sr_population view (the C ABI struct); the Population must outlive
+        its use.  The library binding is imported here, not at module import,
+        so that populations and the workload generators can be used where the
+        library is not loaded (the bench's reference arm)."""
+        from . import _lib
         p = _lib.sr_population()
         p.num_exprs = self.num_exprs
         p.tokens = self.tokens.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
