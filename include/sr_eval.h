@@ -495,6 +495,17 @@ sr_status sr_measure_pipes(sr_context *ctx, double *fp32_ops_per_s,
  * Operators: 0-27 and 32.  No reference counterpart. */
 sr_status sr_measure_operator_rates(sr_context *ctx, const int32_t *ops, int32_t n_ops,
                                    double *evals_per_s);
+/* Accuracy of this library's own single-precision sin / cos / log (the
+ * operators' implementation in every kernel) over the float arguments whose
+ * bit patterns are [begin, begin + count): the largest error in ulps of the
+ * float result against the double-precision function (0.5 = correctly
+ * rounded), the argument where it occurs, and how many checked arguments
+ * were off by more than 0.5 and more than 1 ulp.  fn: 10 sin, 11 cos,
+ * 17 log; 110, 111, 117: CUDA's sinf, cosf, logf for comparison.  Runs on
+ * the current device, synchronous.  No reference counterpart. */
+sr_status sr_check_math(int32_t fn, uint32_t begin, uint64_t count, double *max_ulp,
+                        uint32_t *argmax_bits, uint64_t *checked, uint64_t *over_half_ulp,
+                        uint64_t *over_one_ulp);
 
 #ifdef __cplusplus
 }

@@ -340,9 +340,13 @@ def ref_mark_cached(pop, keys, slots) -> np.ndarray:
 #
 # Maximum errors in ulps of the single-precision functions each side calls,
 # per opcode (IEEE operators are correctly rounded on both sides and carry no
-# entry).  Device: the CUDA Math API's documented maximum ulp errors over the
-# full range (sinf 2, cosf 2, tanf 4, sinhf 3, coshf 2, tanhf 2, expf 2,
-# logf 1, asinf 2, acosf 2, atanf 2, powf 4).  Host: glibc's float functions
+# entry).  Device: sin, cos and log are the library's own (csrc/sr_math.cuh),
+# measured on every float argument of their fast paths against the correctly
+# rounded value (tests/test_gpu_math.py: 1.57, 1.57 and 0.94 ulp; beyond the
+# fast path sin / cos are CUDA's, documented at 2); the others are the CUDA
+# Math API's documented maximum ulp errors over the full range (tanf 4,
+# sinhf 3, coshf 2, tanhf 2, expf 2, asinf 2, acosf 2, atanf 2, powf 4).
+# Host: glibc's float functions
 # (the GNU C Library manual, "Known Maximum Errors in Math Functions", x86_64),
 # taken as 1 ulp for sinf / cosf / expf / logf / powf and 2 for the others,
 # at or above the listed figures.

@@ -170,6 +170,8 @@ _SIGNATURES = {
     "sr_read_grad": (c_int32, [c_void_p, _P(c_float)]),
     "sr_inject_allocation_failure": (c_int32, [c_int64]),
     "sr_measure_operator_rates": (c_int32, [c_void_p, _P(c_int32), c_int32, _P(c_double)]),
+    "sr_check_math": (c_int32, [c_int32, c_uint32, c_uint64, _P(c_double), _P(c_uint32),
+                                _P(c_uint64), _P(c_uint64), _P(c_uint64)]),
     "sr_read_sums": (c_int32, [c_void_p, _P(c_double), _P(c_double)]),
     "sr_read_grad_sums": (c_int32, [c_void_p, _P(c_double)]),
     "sr_device_mse": (c_int32, [c_void_p, _P(c_void_p)]),

@@ -100,17 +100,17 @@ struct VD4 {
     return VD1{o, (DER)};                                            \
   }                                                                  \
   SR_VD1_WIDE(NAME)
-// sin and cos share one argument reduction through sincosf (its two results
-// are bit-identical to sinf / cosf over every float input on sm_100a).
+// sin and cos share one argument reduction through sr_sincosf (its two
+// results are those of sr_sinf / sr_cosf, the forward interpreter's).
 __device__ __forceinline__ VD1 g_sin_body(float x) {
   float s, c;
-  sincosf(x, &s, &c);
+  sr_sincosf(x, &s, &c);
   return VD1{s, c};
 }
 SR_VD1_WIDE(g_sin)
 __device__ __forceinline__ VD1 g_cos_body(float x) {
   float s, c;
-  sincosf(x, &s, &c);
+  sr_sincosf(x, &s, &c);
   return VD1{c, -s};
 }
 SR_VD1_WIDE(g_cos)
@@ -119,12 +119,12 @@ SR_VD1(g_sinh, sinhf(x), coshf(x))
 SR_VD1(g_cosh, coshf(x), sinhf(x))
 SR_VD1(g_tanh, tanhf(x), __fsub_rn(1.0f, __fmul_rn(o, o)))
 SR_VD1(g_exp, expf(x), o)
-SR_VD1(g_log, logf(x), __frcp_rn(x))
+SR_VD1(g_log, sr_logf(x), __frcp_rn(x))
 SR_VD1(g_rcp, __frcp_rn(x), __fmul_rn(-o, o))
 SR_VD1(g_asin, asinf(x), __frcp_rn(__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(x, x)))))
 SR_VD1(g_acos, acosf(x), -__frcp_rn(__fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(x, x)))))
 SR_VD1(g_atan, atanf(x), __frcp_rn(__fadd_rn(1.0f, __fmul_rn(x, x))))
-SR_VD1(g_llog, (x == 0.0f) ? -1e9f : logf(fabsf(x)), (x == 0.0f) ? 0.0f : __frcp_rn(x))
+SR_VD1(g_llog, sr_loose_logf(x), (x == 0.0f) ? 0.0f : __frcp_rn(x))
 SR_VD1(g_linv, __frcp_rn(loose_denom(x)), (fabsf(x) <= 1e-9f) ? 0.0f : __fmul_rn(-o, o))
 SR_VD1(g_sqrt, __fsqrt_rn(x), __frcp_rn(2.0f * o))
 SR_VD1(g_lsqrt, __fsqrt_rn(fabsf(x)), (x == 0.0f) ? 0.0f : signf(x) * __frcp_rn(2.0f * o))

@@ -208,14 +208,14 @@ static_assert(SR_MATH_WIDTH == 1 || SR_MATH_WIDTH == 2 || SR_MATH_WIDTH == 4, "w
     return r;                                                               \
   }
 #endif
-SR_V1(v_sin, sinf(x))
-SR_V1(v_cos, cosf(x))
+SR_V1(v_sin, sr_sinf(x))
+SR_V1(v_cos, sr_cosf(x))
 SR_V1(v_tan, tanf(x))
 SR_V1(v_sinh, sinhf(x))
 SR_V1(v_cosh, coshf(x))
 SR_V1(v_tanh, tanhf(x))
 SR_V1(v_exp, expf(x))
-SR_V1(v_log, logf(x))
+SR_V1(v_log, sr_logf(x))
 SR_V1(v_asin, asinf(x))
 SR_V1(v_acos, acosf(x))
 SR_V1(v_atan, atanf(x))
@@ -511,6 +511,50 @@ constexpr int kInlineMaxDpt = 8;  // wider launches call them (16 copies overflo
               _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = loose_denom(T[k]); \
               SR_MAP2(v_div, T, b, T))
 
+// sin / cos / protected log (this library's own, sr_math.cuh) expanded at
+// their case in the protected profile's switch at up to 8 datapoints per
+// thread.  sin and cos take their fast path for every datapoint of the lane;
+// a lane holding an argument beyond the fast range (|x| > 32768, inf, NaN)
+// evaluates its datapoints through sincos_cold instead (out of line, rare).
+template <int DPT>
+__device__ __noinline__ void sincos_cold(float *T, int q_offset) {
+#pragma unroll
+  for (int k = 0; k < DPT; ++k) T[k] = q_offset ? sr_cosf(T[k]) : sr_sinf(T[k]);
+}
+#define SR_C_SINCOS_INL(CASE, QOFF, NAME)                                      \
+  case CASE:                                                                   \
+    if constexpr (DPT <= kInlineMaxDpt) {                                      \
+      bool slow_ = false;                                                      \
+      _Pragma("unroll") for (int k = 0; k < DPT; ++k) slow_ |= !sincos_fast_ok(T[k]); \
+      if (slow_) {                                                             \
+        float t_[DPT];                                                         \
+        _Pragma("unroll") for (int k = 0; k < DPT; ++k) t_[k] = T[k];          \
+        sincos_cold<DPT>(t_, QOFF);                                            \
+        _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = t_[k];          \
+      } else {                                                                 \
+        _Pragma("unroll") for (int k = 0; k < DPT; ++k) {                      \
+          const float y_ = sincos_pick(sincos_parts(T[k]), QOFF);              \
+          T[k] = (QOFF == 0 && T[k] == 0.0f) ? T[k] : y_;                      \
+        }                                                                      \
+      }                                                                        \
+    } else {                                                                   \
+      SR_MAP1(NAME, T, T)                                                      \
+    }                                                                          \
+    break;
+#define SR_C_SIN_INL SR_C_SINCOS_INL(10, 0, v_sin)
+#define SR_C_COS_INL SR_C_SINCOS_INL(11, 1, v_cos)
+#define SR_C_LLOG_INL                                                          \
+  SR_C_INL_OR(22, T[k] = sr_loose_logf(T[k]),                                  \
+              {                                                                \
+                bool z_[DPT];                                                  \
+                _Pragma("unroll") for (int k = 0; k < DPT; ++k) {              \
+                  z_[k] = (T[k] == 0.0f);                                      \
+                  T[k] = fabsf(T[k]);                                          \
+                }                                                              \
+                SR_MAP1(v_log, T, T)                                           \
+                _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = z_[k] ? -1e9f : T[k]; \
+              })
+
 // Operator profiles (kOpsAll / kOpsProtected and the host-side membership
 // test live in sr_internal.hpp).  kOpsAll dispatches every operator inline;
 // kOpsProtected dispatches + - *, protected division, sin, cos, exp clamped
@@ -581,8 +625,8 @@ template <int DPT, int OPS>
 __device__ __forceinline__ void apply_op(uint32_t op, float (&T)[DPT], float (&b)[DPT]) {
   if constexpr (OPS == kOpsProtected) {
     switch (op) {
-      SR_C_NONE SR_C_ADD SR_C_SUB SR_C_RSUB SR_C_MUL SR_C_LDIV_INL SR_C_RLDIV_INL SR_C_SIN
-      SR_C_COS SR_C_EXPC_INL SR_C_LLOG SR_C_LSQRT_INL
+      SR_C_NONE SR_C_ADD SR_C_SUB SR_C_RSUB SR_C_MUL SR_C_LDIV_INL SR_C_RLDIV_INL SR_C_SIN_INL
+      SR_C_COS_INL SR_C_EXPC_INL SR_C_LLOG_INL SR_C_LSQRT_INL
       SR_C_COLD
     }
   } else {

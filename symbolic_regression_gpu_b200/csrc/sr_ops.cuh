@@ -3,12 +3,15 @@
 // One definition per reference operator, following eval_op_cpu
 // (src/cleaned/cl_cpu_eval.cpp:16-56), which is identical to the reference
 // device version eval_op_gpu_state (src/cleaned/cl_gpu_eval.cu:14-54):
-// x is the first popped (left) operand, y the second.  The CUDA math library
-// functions are called as they are; IEEE-rounded intrinsics are spelled out
-// for the basic operations so no contraction into FMA can change a result.
+// x is the first popped (left) operand, y the second.  sin, cos and log are
+// this library's own (sr_math.cuh); the other functions are the CUDA math
+// library's, called as they are; IEEE-rounded intrinsics are spelled out for
+// the basic operations so no contraction into FMA can change a result.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include "sr_math.cuh"
 
 namespace sr {
 
@@ -39,19 +42,19 @@ __device__ __forceinline__ float op_binary(int op, float x, float y) {
 __device__ __forceinline__ float op_unary(int op, float x) {
   switch (op) {
     case 0: return x;  // MOV (bytecode only)
-    case 10: return sinf(x);
-    case 11: return cosf(x);
+    case 10: return sr_sinf(x);
+    case 11: return sr_cosf(x);
     case 12: return tanf(x);
     case 13: return sinhf(x);
     case 14: return coshf(x);
     case 15: return tanhf(x);
     case 16: return expf(x);
-    case 17: return logf(x);
+    case 17: return sr_logf(x);
     case 18: return __frcp_rn(x);
     case 19: return asinf(x);
     case 20: return acosf(x);
     case 21: return atanf(x);
-    case 22: return (x == 0.0f) ? -1e9f : logf(fabsf(x));
+    case 22: return sr_loose_logf(x);
     case 23: return __frcp_rn(loose_denom(x));
     case 24: return fabsf(x);
     case 25: return -x;
