@@ -353,16 +353,16 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
                                              const float *xs, int xrs, const SpillStack &st,
                                              int lane, const float *cache, int64_t ldc,
                                              int64_t dp0) {
-  if (kind == kBC) {
+  if (kind == kBX) {
+    lds_vec<DPT>(xs + payload * xrs, lane, b);
+  } else if (kind == kBS) {
+    spill_load<DPT>(st, payload, lane, b);
+  } else if (!CACHE || kind == kBC) {
     const float c = __uint_as_float(payload);
 #pragma unroll
     for (int k = 0; k < DPT; ++k) b[k] = c;
-  } else if (CACHE && kind == kBR) {
-    ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, b);
-  } else if (kind == kBX) {
-    lds_vec<DPT>(xs + payload * xrs, lane, b);
   } else {
-    spill_load<DPT>(st, payload, lane, b);
+    ldg_vec<DPT>(cache + static_cast<int64_t>(payload) * ldc + dp0, lane, b);
   }
 }
 
@@ -532,9 +532,12 @@ __device__ __noinline__ void sincos_cold(float *T, int q_offset) {
         sincos_cold<DPT>(t_, QOFF);                                            \
         _Pragma("unroll") for (int k = 0; k < DPT; ++k) T[k] = t_[k];          \
       } else {                                                                 \
-        _Pragma("unroll") for (int k = 0; k < DPT; ++k) {                      \
-          const float y_ = sincos_pick(sincos_parts(T[k]), QOFF);              \
-          T[k] = (QOFF == 0 && T[k] == 0.0f) ? T[k] : y_;                      \
+        _Pragma("unroll") for (int k = 0; k < DPT; k += 2) {                   \
+          SinCosParts p0_, p1_;                                                \
+          sincos_parts2(make_float2(T[k], T[k + 1]), p0_, p1_);                \
+          const float y0_ = sincos_pick(p0_, QOFF), y1_ = sincos_pick(p1_, QOFF); \
+          T[k] = (QOFF == 0 && T[k] == 0.0f) ? T[k] : y0_;                     \
+          T[k + 1] = (QOFF == 0 && T[k + 1] == 0.0f) ? T[k + 1] : y1_;         \
         }                                                                      \
       }                                                                        \
     } else {                                                                   \
@@ -544,7 +547,11 @@ __device__ __noinline__ void sincos_cold(float *T, int q_offset) {
 #define SR_C_SIN_INL SR_C_SINCOS_INL(10, 0, v_sin)
 #define SR_C_COS_INL SR_C_SINCOS_INL(11, 1, v_cos)
 #define SR_C_LLOG_INL                                                          \
-  SR_C_INL_OR(22, T[k] = sr_loose_logf(T[k]),                                  \
+  SR_C_INL_OR(22, if ((k & 1) == 0) {                                          \
+                const float2 l_ = sr_log_nonneg2(fabsf(T[k]), fabsf(T[k + 1])); \
+                T[k] = T[k] == 0.0f ? -1e9f : l_.x;                            \
+                T[k + 1] = T[k + 1] == 0.0f ? -1e9f : l_.y;                    \
+              },                                                               \
               {                                                                \
                 bool z_[DPT];                                                  \
                 _Pragma("unroll") for (int k = 0; k < DPT; ++k) {              \
@@ -655,9 +662,11 @@ __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
     // the next word is always in bounds.
     const uint4 nxt = ldg_instr(code + i + 1);
     const uint32_t w = ins.x;
-    if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
-    if (instr_load(w))
-      load_leaf<DPT, CACHE>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
+    if (w & (kLoadBit | kSpillBit)) {
+      if (instr_spill(w)) spill_store<DPT>(st, instr_spill_slot(w), lane, T);
+      if (instr_load(w))
+        load_leaf<DPT, CACHE>(instr_leaf_kind(w), ins.y, T, xs, xrs, lane, cache, ldc, dp0);
+    }
     float b[DPT];
     const uint32_t bk = instr_b_kind(w);
     if (bk != kBNone) load_operand<DPT, CACHE>(bk, ins.z, b, xs, xrs, st, lane, cache, ldc, dp0);
@@ -667,7 +676,7 @@ __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
 }
 
 // Sum of the valid squared errors of a lane's DPT datapoints in FP64: the
-// fallback when the FP32 Kahan sum overflowed (or a square is infinite); exact
+// fallback when the FP32 tile sum overflowed (or a square is infinite); exact
 // for DPT finite squares and +Inf when one is infinite, like the reference's
 // double sum.  Out of line: it almost never runs.
 template <int DPT>

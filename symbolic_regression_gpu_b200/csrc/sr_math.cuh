@@ -20,6 +20,11 @@
 //     script), ln2 split in two so that e * ln2_hi is exact; subnormal
 //     arguments are scaled by 2^23 first.
 //
+// The interpreter evaluates two datapoints at once with the paired FP32
+// instructions of sm_100 (fma.rn.f32x2 and friends: sincos_parts2,
+// sr_log_nonneg2); each half is the same correctly rounded operation as the
+// scalar form, so both forms give identical results.
+//
 // Their accuracy is measured on every float argument against the correctly
 // rounded value (sr_check_math, tests/test_gpu_math.py) and is the device
 // column of the parity rule's error table.  Every kernel of this library that
@@ -114,6 +119,29 @@ __device__ __forceinline__ void sr_sincosf(float x, float *s, float *c) {
   *c = sincos_pick(p, 1);
 }
 
+// Two arguments at once in paired FP32 operations (fma.rn.f32x2 and friends:
+// each half is the same correctly rounded operation as the scalar form, so
+// the results are those of sincos_parts).
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ void sincos_parts2(float2 x, SinCosParts &p0, SinCosParts &p1) {
+  const float2 t = __ffma2_rn(x, f2(kTwoOverPi), f2(kRoundMagic));
+  const float2 j = __fadd2_rn(t, f2(-kRoundMagic));
+  p0.q = __float_as_int(t.x);
+  p1.q = __float_as_int(t.y);
+  float2 r = __ffma2_rn(j, f2(-kPio2Hi), x);
+  r = __ffma2_rn(j, f2(-kPio2Mid), r);
+  r = __ffma2_rn(j, f2(-kPio2Lo), r);
+  const float2 z = __fmul2_rn(r, r);
+  float2 ps = __ffma2_rn(f2(kS2), z, f2(kS1));
+  ps = __ffma2_rn(ps, z, f2(kS0));
+  const float2 s = __ffma2_rn(__fmul2_rn(r, z), ps, r);
+  float2 pc = __ffma2_rn(f2(kC2), z, f2(kC1));
+  pc = __ffma2_rn(pc, z, f2(kC0));
+  pc = __ffma2_rn(pc, z, f2(-0.5f));
+  const float2 c = __ffma2_rn(z, pc, f2(1.0f));
+  p0.s = s.x; p1.s = s.y; p0.c = c.x; p1.c = c.y;
+}
+
 // log(1 + f) = f + f^2 (-1/2 + f R(f)), R(f) = kR0 + f (kR1 + ... f kR7)
 constexpr float kR0 = 0.333333317078f;
 constexpr float kR1 = -0.250008210321f;
@@ -150,6 +178,32 @@ __device__ __forceinline__ float sr_log_nonneg(float a) {
   const float y = fmaf(__fmul_rn(f, f), p, f);
   const float r = fmaf(ef, kLn2Hi, fmaf(ef, kLn2Lo, y));
   return (a == 0.0f) ? __int_as_float(0xff800000) : (a < INFINITY ? r : a);
+}
+
+// sr_log_nonneg of two arguments, the polynomial in paired operations.
+__device__ __forceinline__ float2 sr_log_nonneg2(float a0, float a1) {
+  const bool sub0 = a0 < 1.17549435e-38f, sub1 = a1 < 1.17549435e-38f;
+  const float as0 = sub0 ? __fmul_rn(a0, 8388608.0f) : a0;
+  const float as1 = sub1 ? __fmul_rn(a1, 8388608.0f) : a1;
+  const int ia0 = __float_as_int(as0), ia1 = __float_as_int(as1);
+  const int e0 = (ia0 - 0x3f3504f3) >> 23, e1 = (ia1 - 0x3f3504f3) >> 23;
+  const float2 m = make_float2(__int_as_float(ia0 - (e0 << 23)), __int_as_float(ia1 - (e1 << 23)));
+  const float2 f = __fadd2_rn(m, f2(-1.0f));
+  const float2 ef = make_float2(static_cast<float>(sub0 ? e0 - 23 : e0),
+                                static_cast<float>(sub1 ? e1 - 23 : e1));
+  float2 p = __ffma2_rn(f2(kR7), f, f2(kR6));
+  p = __ffma2_rn(p, f, f2(kR5));
+  p = __ffma2_rn(p, f, f2(kR4));
+  p = __ffma2_rn(p, f, f2(kR3));
+  p = __ffma2_rn(p, f, f2(kR2));
+  p = __ffma2_rn(p, f, f2(kR1));
+  p = __ffma2_rn(p, f, f2(kR0));
+  p = __ffma2_rn(p, f, f2(-0.5f));
+  const float2 y = __ffma2_rn(__fmul2_rn(f, f), p, f);
+  const float2 r = __ffma2_rn(ef, f2(kLn2Hi), __ffma2_rn(ef, f2(kLn2Lo), y));
+  return make_float2(
+      (a0 == 0.0f) ? __int_as_float(0xff800000) : (a0 < INFINITY ? r.x : a0),
+      (a1 == 0.0f) ? __int_as_float(0xff800000) : (a1 < INFINITY ? r.y : a1));
 }
 
 // logf semantics: NaN for negative arguments.
