@@ -83,6 +83,14 @@ def parse_args():
     return ap.parse_args()
 
 
+_T0 = time.perf_counter()
+
+
+def _progress(what: str):
+    """One progress line on stderr (stdout carries only the JSON result)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {what}", file=sys.stderr, flush=True)
+
+
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
             int(os.environ.get("WORLD_SIZE", "1")))
@@ -699,6 +707,7 @@ def run_ours(args):
     sr_stream = torch.cuda.ExternalStream(ev.stream_handle, device=dev)
     ev.set_data(w.X)
     ev.prepare(w.population)  # compile + upload + shape tuning (outside timing)
+    _progress("headline population prepared")
     node_evals = w.population.num_tokens * w.num_dps
 
     def step():
@@ -734,6 +743,7 @@ def run_ours(args):
     if world > 1:
         torch.distributed.barrier()
     clk = clocks.stop()
+    _progress("headline steps timed")
     total_ms = sum(step_ms)
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
@@ -798,21 +808,26 @@ def run_ours(args):
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args)
+        _progress("forward+adjoint figures")
 
     cache = None
     if not args.no_cache_figures:
         cache = cache_figures(ev, rank, flush_buf, sr_stream, args)
+        _progress("subtree-cache figures")
     evolution = None
     if not args.no_evolution:
         evolution = evolution_figures(ev, w, torch, sr_stream)
+        _progress("device evolution figures")
     large = None
     if not args.no_large:
         large = large_figures(ev, rank, flush_buf, sr_stream)
+        _progress("large population figures")
         ev.set_data(w.X)
     plain_config = None
     if not args.no_plain_config and rank == 0 and world == 1:
         plain_config = plain_config_figures(ev, torch, flush_buf, sr_stream,
                                             os.cpu_count() or 1)
+        _progress("plain workload figures")
         ev.set_data(w.X)
 
     # End to end through the public API: pinned host dataset and host
@@ -842,6 +857,7 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_value = node_evals * world / e2e_s
+    _progress("end-to-end steps")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -867,14 +883,17 @@ def run_ours(args):
                         "finite": int(r.size)}
             cpu["accuracy_vs_fp64"] = {"reference_cpu": _stats(ref_mse),
                                        "this_gpu_same_expressions": _stats(mse[idx])}
+            _progress("CPU baseline")
             cpu["parity"] = parity_figures(ev, w, sample, mse[idx], ref_mse,
                                            os.cpu_count() or 1, cpu.pop("_patched"))
+            _progress("parity figures")
 
     reference_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ev.synchronize()
         try:
             reference_gpu = reference_gpu_figures(w)
+            _progress("reference GPU figures")
         except (ImportError, OSError, subprocess.SubprocessError) as ex:
             reference_gpu = {"unavailable": str(ex)}
         if "kernel_node_evals_per_s" in reference_gpu.get("simple", {}):
