@@ -491,8 +491,8 @@ __global__ void __launch_bounds__((kMaxWarps + 1) * 32, 1) adj_kernel(const AdjA
   const int n_items = p.n_groups * p.n_spans;
   if (warp == W) {
     if (lane == 0)
-      run_producer(p.n_groups, n_items, p.work_counter, p.error, p.X, p.ldx, rows, span, xbuf,
-                   desc, full, empty);
+      run_producer<false>(p.n_groups, n_items, 1, p.n_spans, p.work_counter, p.error, p.X,
+                          p.ldx, rows, span, xbuf, desc, full, empty, FoldArgs{});
     return;
   }
 

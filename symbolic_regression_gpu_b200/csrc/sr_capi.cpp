@@ -201,7 +201,7 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
   // Span: the target, shrunk to the data and to the shared-memory budget.
   int64_t span = std::min<int64_t>(span_target, std::max<int64_t>(tile, round_up(ctx->N, tile)));
   while (span > tile &&
-         sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, static_cast<int>(span)) >
+         sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, static_cast<int>(span), p.G, pred) >
              static_cast<size_t>(dev_max_smem))
     span = std::max<int64_t>(tile, (span / 2) / tile * tile);
   // Then, while the span's shared memory (the X buffers grow with the
@@ -212,13 +212,15 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
     int bps_now = 0;
     SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache,
                                           sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem,
-                                                                static_cast<int>(span)),
+                                                                static_cast<int>(span), p.G,
+                                                                pred),
                                           W, &bps_now));
     while (span / 2 >= std::max<int64_t>(tile, kMinSpan) && (span / 2) % tile == 0) {
       int bps_half = 0;
       SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache,
                                             sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem,
-                                                                  static_cast<int>(span / 2)),
+                                                                  static_cast<int>(span / 2),
+                                                                  p.G, pred),
                                             W, &bps_half));
       if (bps_half <= bps_now) break;
       span /= 2;
@@ -228,16 +230,26 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
   // The kernel walks a span tile by tile: it must hold whole tiles.
   if (span % tile != 0) return ctx->fail(SR_ERR_UNSUPPORTED, "span is not a multiple of the tile");
   p.span = static_cast<int>(span);
-  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, p.span);
+  p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, p.span, p.G, pred);
   if (p.smem > static_cast<size_t>(dev_max_smem))
     return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape needs " + std::to_string(p.smem) +
                                              " bytes of shared memory");
   p.n_spans = (ctx->N == 0 || E == 0) ? 0 : static_cast<int>((ctx->N + span - 1) / span);
-  // One FP64 (sum, count) per (span, expression): 16 B x E x N / span.  It is
-  // sized against the device's memory (the allocation itself reports
-  // SR_ERR_OUT_OF_MEMORY when the free memory is short).
+  // Spans per work item: as many as keep about 32 items per SM (up to 32
+  // spans), so the per-(span group, expression) entries stay small while the
+  // items still balance over the SMs.  The result does not depend on this
+  // choice (the spans' sums are added as double-doubles).
+  p.k_spans = 1;
+  if (!pred && p.n_spans > 0) {
+    const int64_t per_sm = static_cast<int64_t>(p.n_spans) * p.n_groups /
+                           (32 * static_cast<int64_t>(std::max(ctx->num_sms, 1)));
+    p.k_spans = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(32, per_sm)));
+  }
+  // One FP64 (sum as hi + lo, count) per (span group, expression): 32 B x E
+  // x span groups.  It is sized against the device's memory (the allocation
+  // itself reports SR_ERR_OUT_OF_MEMORY when the free memory is short).
   if (!pred) {
-    const double need = static_cast<double>(p.n_spans) * E * 16.0;
+    const double need = static_cast<double>(p.n_span_groups()) * E * 32.0;
     if (need > 0.9 * static_cast<double>(ctx->device_memory))
       return ctx->fail(SR_ERR_UNSUPPORTED,
                        "partial-sum buffer (" + std::to_string(static_cast<int64_t>(need)) +
@@ -320,6 +332,7 @@ sr::EvalArgs make_args(sr_context *ctx, ProgramSet &ps, int32_t *counter) {
   a.n_spans = ps.plan.n_spans;
   a.spill = ctx->spill.p;
   a.s_smem = ps.plan.s_smem;
+  a.span_per_item = ps.plan.k_spans;
   return a;
 }
 
@@ -399,7 +412,8 @@ static sr_status time_shape(sr_context *ctx, int dpt, int W, int split, int per_
   }
   SR_TRY(upload_groups(ctx, ctx->main));
   SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(std::max<int64_t>(
-                       static_cast<int64_t>(ctx->main.plan.n_spans) * ctx->main.E, 1))));
+                       2 * static_cast<int64_t>(ctx->main.plan.n_span_groups()) * ctx->main.E,
+                       1))));
   cudaEvent_t a = ctx->ev[4], b = ctx->ev[5];
   float t_sum = 0.f;
   for (int rep = 0; rep < 3; ++rep) {
@@ -495,8 +509,8 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
   if (ctx->opts.smem_spill_slots >= 0) split = ctx->opts.smem_spill_slots;
   SR_TRY(plan_set(ctx, ps, false, dpt, W, split, per_warp));
   SR_TRY(upload_groups(ctx, ps));
-  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
-                       std::max<int64_t>(static_cast<int64_t>(ps.plan.n_spans) * ps.E, 1))));
+  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(std::max<int64_t>(
+                       2 * static_cast<int64_t>(ps.plan.n_span_groups()) * ps.E, 1))));
   return SR_OK;
 }
 
@@ -1091,8 +1105,8 @@ static sr_status enqueue_launch(sr_context *ctx, int *launches_out) {
       ++launches;
     }
     SR_TRY_CUDA(ctx, record_event(ctx, 2));
-    SR_TRY_CUDA(ctx, sr::launch_finalize(ctx->partial.p, ctx->main.plan.n_spans, ctx->E,
-                                         ctx->mse.p, s));
+    SR_TRY_CUDA(ctx, sr::launch_finalize_groups(ctx->partial.p, ctx->main.plan.n_span_groups(),
+                                                ctx->E, ctx->mse.p, nullptr, s));
     ++launches;
   }
   SR_TRY_CUDA(ctx, record_event(ctx, 3));
@@ -1217,14 +1231,18 @@ sr_status sr_read_sums(sr_context *ctx, double *sum_out, double *count_out) {
   switch (ctx->mode) {
     case sr::Mode::kPlain: n_spans = ctx->N > 0 ? ctx->plain.n_dpblocks : 0; break;
     case sr::Mode::kGrad: n_spans = ctx->grad.n_spans; break;
-    default: n_spans = ctx->main.plan.n_spans; break;
+    default: n_spans = ctx->main.plan.n_span_groups(); break;
   }
   const int E = ctx->E;
   DeviceScope scope(ctx->device);
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the buffers may grow
   SR_TRY_CUDA(ctx, ctx->sums.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ctx->h_sums.ensure(static_cast<size_t>(E)));
-  SR_TRY_CUDA(ctx, sr::launch_sums(ctx->partial.p, n_spans, E, ctx->sums.p, ctx->stream));
+  if (ctx->mode == sr::Mode::kPlain || ctx->mode == sr::Mode::kGrad)
+    SR_TRY_CUDA(ctx, sr::launch_sums(ctx->partial.p, n_spans, E, ctx->sums.p, ctx->stream));
+  else
+    SR_TRY_CUDA(ctx, sr::launch_finalize_groups(ctx->partial.p, n_spans, E, nullptr,
+                                                ctx->sums.p, ctx->stream));
   SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_sums.p, ctx->sums.p, E * sizeof(double2),
                                    cudaMemcpyDeviceToHost, ctx->stream));
   SR_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->h_error, ctx->d_error, sizeof(int32_t),

@@ -104,9 +104,11 @@ struct Plan {
   int n_groups = 0;
   int span = 0;        // datapoints per span
   int n_spans = 0;
+  int k_spans = 1;     // spans per work item (EvalArgs::span_per_item)
   int blocks = 0;
   size_t smem = 0;
-  int64_t items() const { return static_cast<int64_t>(n_groups) * n_spans; }
+  int n_span_groups() const { return (n_spans + k_spans - 1) / k_spans; }
+  int64_t items() const { return static_cast<int64_t>(n_groups) * n_span_groups(); }
 };
 
 // A compiled population resident on the device.

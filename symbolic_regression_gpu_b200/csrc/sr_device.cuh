@@ -692,47 +692,153 @@ __device__ __noinline__ double tile_sum_fp64(const float *T, const float *y, boo
   return sum;
 }
 
-// The producer thread of a block: claims work items (span, group) from the
-// global counter and copies each item's X span (every row) into one of kBufs
-// shared-memory buffers with the bulk-copy engine; publishes item -1 when
-// the work runs out.  Every wait is bounded.
-__device__ __noinline__ void run_producer(int n_groups, int n_items, int32_t *work_counter,
-                                          int32_t *error, const float *X, int64_t ldx,
-                                          int rows, int span, float *xbuf, ItemDesc *desc,
-                                          uint64_t *full, uint64_t *empty) {
+// Per-span result of one expression of a work item, written by the warp that
+// evaluated it (shared memory, one slot per buffer and group position).
+struct SpanPart {
+  double sum;   // sum of the valid squared errors over the span
+  int32_t cnt;  // valid datapoints
+  int32_t e;    // expression
+};
+
+// Per-item accumulator of one expression (producer thread only): the span
+// sums added in span order as a double-double (hi + lo, Knuth's two-sum), so
+// that the result does not depend on how many spans an item covers.
+struct GroupAcc {
+  double hi, lo, cnt;
+  int32_t e, pad;
+};
+
+__device__ __forceinline__ void dd_add(double &hi, double &lo, double x) {
+  const double s = __dadd_rn(hi, x);
+  if (isfinite(s)) {
+    const double bb = __dsub_rn(s, hi);
+    lo = __dadd_rn(lo, __dadd_rn(__dsub_rn(hi, __dsub_rn(s, bb)), __dsub_rn(x, bb)));
+  } else {
+    lo = 0.0;  // an infinite sum stays infinite
+  }
+  hi = s;
+}
+
+// What the producer of an MSE launch folds: the span slots, its accumulators
+// and where a finished item's sums go ([span group][E] entries of two
+// double2: (hi, lo) and (count, 0)).
+struct FoldArgs {
+  SpanPart *part;  // [kBufs][G]
+  GroupAcc *acc;   // [G]
+  double2 *out;
+  int G, E;
+};
+
+// The producer thread of a block: claims work items from the global counter
+// (item = span group x expression group; single-span items are numbered
+// span-major, so concurrent blocks share X spans in L2; multi-span items
+// expression-group-major, so the most expensive groups, which come first in
+// the cost-sorted group table, are claimed first and the last items are the
+// cheapest), and copies each of the item's spans
+// (k_spans consecutive spans, the last group shorter) with every row of X
+// into one of kBufs shared-memory buffers with the bulk-copy engine;
+// publishes item -1 when the work runs out.  With FOLD (MSE launches) it also
+// folds, once the warps have released a buffer, the span slots written for it
+// into the item's accumulators (in span order) and writes each finished
+// item's sums out.  Every wait is bounded.
+template <bool FOLD>
+__device__ __noinline__ void run_producer(int n_groups, int n_items, int k_spans, int n_spans,
+                                          int32_t *work_counter, int32_t *error, const float *X,
+                                          int64_t ldx, int rows, int span, float *xbuf,
+                                          ItemDesc *desc, uint64_t *full, uint64_t *empty,
+                                          FoldArgs fa) {
   uint32_t buf = 0, phase = 0;
   uint32_t armed = 0;  // buffers with a copy in flight
-  uint32_t armed_parity0 = 0, armed_parity1 = 0;
+  uint32_t fill_phase[kBufs] = {0, 0};
+  bool held[kBufs] = {false, false};  // a span whose slots are still to fold
+  int held_item[kBufs] = {0, 0}, held_group[kBufs] = {0, 0};
+  int acc_item = -1, acc_sg = 0, acc_n = 0;
   const uint32_t row_bytes = static_cast<uint32_t>(span) * sizeof(float);
+
+  auto flush = [&]() {
+    if (!FOLD || acc_item < 0) return;
+    for (int j = 0; j < acc_n; ++j) {
+      const GroupAcc a = fa.acc[j];
+      double2 *o = fa.out + 2 * (static_cast<int64_t>(acc_sg) * fa.E + a.e);
+      o[0] = make_double2(a.hi, a.lo);
+      o[1] = make_double2(a.cnt, 0.0);
+    }
+    acc_item = -1;
+  };
+  auto fold = [&](uint32_t b) {
+    if (!FOLD) return;
+    const int it = held_item[b];
+    if (it != acc_item) {
+      flush();
+      acc_item = it;
+      acc_sg = k_spans > 1 ? it % ((n_spans + k_spans - 1) / k_spans) : it / n_groups;
+      const int g = held_group[b];
+      acc_n = min(fa.G, fa.E - g * fa.G);  // groups are padded at their end only
+      for (int j = 0; j < acc_n; ++j) fa.acc[j] = GroupAcc{0.0, 0.0, 0.0, 0, 0};
+    }
+    const SpanPart *q = fa.part + static_cast<size_t>(b) * fa.G;
+    for (int j = 0; j < acc_n; ++j) {
+      const SpanPart v = q[j];
+      dd_add(fa.acc[j].hi, fa.acc[j].lo, v.sum);
+      fa.acc[j].cnt += static_cast<double>(v.cnt);
+      fa.acc[j].e = v.e;
+    }
+    held[b] = false;
+  };
+  auto drain = [&]() {
+    // Let copies already issued land before the block exits.
+    if (armed & 1u) mbar_drain(&full[0], fill_phase[0]);
+    if (armed & 2u) mbar_drain(&full[1], fill_phase[1]);
+  };
+
   for (;;) {
     const int item = atomicAdd(work_counter, 1);
-    if (!mbar_wait(&empty[buf], phase ^ 1u, error)) {
-      // Let copies already issued land before the block exits.
-      if (armed & 1u) mbar_drain(&full[0], armed_parity0);
-      if (armed & 2u) mbar_drain(&full[1], armed_parity1);
-      return;
-    }
-    // The consumers released this buffer, so its previous copy landed.
-    armed &= ~(1u << buf);
-    if (item >= n_items) {
-      desc[buf] = ItemDesc{-1, 0, 0, 0};
-      mbar_arrive(&full[buf]);
-      return;
-    }
-    const int group = item % n_groups;
-    const int sp = item / n_groups;
-    desc[buf] = ItemDesc{item, group, sp, 0};
-    mbar_arrive_expect_tx(&full[buf], row_bytes * rows);
-    const float *src = X + static_cast<int64_t>(sp) * span;
-    float *dst = xbuf + static_cast<size_t>(buf) * rows * span;
-    for (int v = 0; v < rows; ++v)
-      bulk_g2s(dst + static_cast<size_t>(v) * span, src + v * ldx, row_bytes, &full[buf]);
-    armed |= 1u << buf;
-    if (buf == 0) armed_parity0 = phase;
-    else armed_parity1 = phase;
-    if (++buf == kBufs) {
-      buf = 0;
-      phase ^= 1u;
+    const bool last = item >= n_items;
+    const int n_sg = (n_spans + k_spans - 1) / k_spans;
+    const int group = last ? 0 : (k_spans > 1 ? item / n_sg : item % n_groups);
+    const int sgi = last ? 0 : (k_spans > 1 ? item % n_sg : item / n_groups);
+    const int s_begin = sgi * k_spans;
+    const int s_end = last ? 1 : min(n_spans, s_begin + k_spans);
+    for (int sp = s_begin; sp < s_end; ++sp) {
+      if (!mbar_wait(&empty[buf], phase ^ 1u, error)) {
+        drain();
+        return;
+      }
+      // The consumers released this buffer, so its previous copy landed and
+      // its span slots are complete.
+      armed &= ~(1u << buf);
+      if (held[buf]) fold(buf);
+      if (last) {
+        desc[buf] = ItemDesc{-1, 0, 0, 0};
+        mbar_arrive(&full[buf]);
+        if (FOLD) {
+          const uint32_t other = buf ^ 1u;
+          if (held[other]) {
+            if (!mbar_wait(&empty[other], fill_phase[other], error)) {
+              drain();
+              return;
+            }
+            fold(other);
+          }
+          flush();
+        }
+        return;
+      }
+      desc[buf] = ItemDesc{item, group, sp, 0};
+      mbar_arrive_expect_tx(&full[buf], row_bytes * rows);
+      const float *src = X + static_cast<int64_t>(sp) * span;
+      float *dst = xbuf + static_cast<size_t>(buf) * rows * span;
+      for (int v = 0; v < rows; ++v)
+        bulk_g2s(dst + static_cast<size_t>(v) * span, src + v * ldx, row_bytes, &full[buf]);
+      armed |= 1u << buf;
+      fill_phase[buf] = phase;
+      held[buf] = FOLD;
+      held_item[buf] = item;
+      held_group[buf] = group;
+      if (++buf == kBufs) {
+        buf = 0;
+        phase ^= 1u;
+      }
     }
   }
 }

@@ -121,7 +121,7 @@ struct EvalArgs {
   const int64_t *code_off;   // [E] first instruction of each expression
   const int32_t *code_len;   // [E] instruction count
   const int32_t *group_expr; // [n_groups * G] expression index or -1 (tail)
-  double2 *partial;      // [n_spans][E] (sum of squared errors, valid count)
+  double2 *partial;      // [n_span_groups][E] x 2 (MSE launches; see span_per_item)
   int32_t *work_counter; // zeroed before each launch
   int32_t *error;        // device error word
   const float *cache;    // subtree cache [slot][ldc] (cached-subtree operands)
@@ -142,7 +142,11 @@ struct EvalArgs {
   // (blockIdx.x * W + warp), (smax - s_smem) tiles of 32*DPT floats.
   float *spill;
   int32_t s_smem;
-  int32_t reserved0;
+  // Spans per work item: an item is (span group, expression group), a span
+  // group k_spans consecutive spans.  MSE launches write one entry per (span
+  // group, expression) into `partial`: two double2, (sum as hi + lo,
+  // count).
+  int32_t span_per_item;
 };
 
 }  // namespace sr

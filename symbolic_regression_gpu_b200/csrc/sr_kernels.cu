@@ -64,6 +64,8 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
       reinterpret_cast<ItemDesc *>(sreg + static_cast<size_t>(W) * p.s_smem * TILE);
   uint64_t *full = reinterpret_cast<uint64_t *>(desc + kBufs);
   uint64_t *empty = full + kBufs;
+  SpanPart *part = reinterpret_cast<SpanPart *>(empty + kBufs);  // MSE launches only
+  GroupAcc *gacc = reinterpret_cast<GroupAcc *>(part + kBufs * p.G);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kBufs; ++s) {
@@ -74,12 +76,14 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
   }
   __syncthreads();
 
-  const int n_items = p.n_groups * p.n_spans;
+  const int k_spans = p.span_per_item;
+  const int n_items = p.n_groups * ((p.n_spans + k_spans - 1) / k_spans);
 
   if (warp == W) {
     if (lane == 0)
-      run_producer(p.n_groups, n_items, p.work_counter, p.error, p.X, p.ldx, rows, span, xbuf,
-                   desc, full, empty);
+      run_producer<!PRED>(p.n_groups, n_items, k_spans, p.n_spans, p.work_counter, p.error, p.X,
+                          p.ldx, rows, span, xbuf, desc, full, empty,
+                          FoldArgs{part, gacc, p.partial, p.G, p.E});
     return;
   }
 
@@ -178,9 +182,7 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
           acc += __shfl_xor_sync(0xffffffffu, acc, o);
           cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         }
-        if (lane == 0)
-          p.partial[static_cast<int64_t>(d.span) * p.E + e] =
-              make_double2(acc, static_cast<double>(cnt));
+        if (lane == 0) part[static_cast<size_t>(buf) * p.G + j] = SpanPart{acc, cnt, e};
       }
     }
     __syncwarp();
@@ -190,6 +192,26 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
       phase ^= 1u;
     }
   }
+}
+
+// The same for the interpreter's entries ([n_groups][E] x (hi, lo), (count,
+// 0)): the span groups' double-double sums added in order, then mse =
+// (hi + lo) / count.
+__global__ void finalize_dd_kernel(const double2 *__restrict__ partial, int n_groups, int E,
+                                   float *__restrict__ mse, double2 *__restrict__ sums) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  double hi = 0.0, lo = 0.0, c = 0.0;
+  for (int k = 0; k < n_groups; ++k) {
+    const double2 *q = partial + 2 * (static_cast<int64_t>(k) * E + e);
+    const double2 a = q[0];
+    dd_add(hi, lo, a.x);
+    dd_add(hi, lo, a.y);
+    c += q[1].x;
+  }
+  const double s = isfinite(hi) ? __dadd_rn(hi, lo) : hi;
+  if (mse) mse[e] = (c > 0.0) ? static_cast<float>(s / c) : qnan();
+  if (sums) sums[e] = make_double2(s, c);
 }
 
 __global__ void finalize_kernel(const double2 *__restrict__ partial, int n_spans,
@@ -465,11 +487,12 @@ using OpRates = OpRateTable<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15
 
 }  // namespace
 
-size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span) {
+size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span, int G, bool pred) {
   const size_t tile = 32u * static_cast<size_t>(dpt);
   return (static_cast<size_t>(kBufs) * (V + 1) * span +
           static_cast<size_t>(W) * s_smem * tile) * sizeof(float) +
-         kBufs * sizeof(ItemDesc) + 2 * kBufs * sizeof(uint64_t);
+         kBufs * sizeof(ItemDesc) + 2 * kBufs * sizeof(uint64_t) +
+         (pred ? 0 : static_cast<size_t>(G) * (kBufs * sizeof(SpanPart) + sizeof(GroupAcc)));
 }
 
 template <int DPT, bool PRED, int MAXW, int MINB, int OPS = kOpsAll, bool CACHE = false>
@@ -536,6 +559,13 @@ cudaError_t launch_finalize(const double2 *partial, int n_spans, int E,
                             float *mse, cudaStream_t stream) {
   if (E <= 0) return cudaSuccess;
   finalize_kernel<<<(E + 255) / 256, 256, 0, stream>>>(partial, n_spans, E, mse);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_groups(const double2 *partial, int n_groups, int E, float *mse,
+                                   double2 *sums, cudaStream_t stream) {
+  if (E <= 0) return cudaSuccess;
+  finalize_dd_kernel<<<(E + 255) / 256, 256, 0, stream>>>(partial, n_groups, E, mse, sums);
   return cudaGetLastError();
 }
 

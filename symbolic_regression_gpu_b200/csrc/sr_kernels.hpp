@@ -15,7 +15,7 @@ constexpr int kPlainStack = 128;                    // plain kernel stack depth
 constexpr int kFp64Stack = 96;                      // FP64 reference kernel stack depth
 
 // Dynamic shared memory of interp_kernel for a launch shape.
-size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span);
+size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span, int G, bool pred);
 // Spill slots per warp kept in shared memory for a datapoints-per-thread
 // choice (deeper slots go to global scratch).
 inline int smem_spill_slots(int dpt) { return dpt >= 16 ? 2 : (dpt == 8 ? 4 : 8); }
@@ -29,8 +29,14 @@ cudaError_t launch_interp(int dpt, bool pred, int ops, bool cache, const EvalArg
                           int blocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_finalize(const double2 *partial, int n_spans, int E,
                             float *mse, cudaStream_t stream);
+// The interpreter's MSE entries ([n_groups][E] x 2 double2 per span group,
+// see EvalArgs::span_per_item): mse = sum / count (NaN without a valid
+// datapoint) into `mse`, and (sum, count) into `sums`; either may be NULL.
+cudaError_t launch_finalize_groups(const double2 *partial, int n_groups, int E, float *mse,
+                                   double2 *sums, cudaStream_t stream);
 // (sum of valid squared errors, valid count) per expression, combined over
-// the span partials in the order launch_finalize uses.
+// the span partials in the order launch_finalize uses (plain and gradient
+// launches).
 cudaError_t launch_sums(const double2 *partial, int n_spans, int E, double2 *sums,
                         cudaStream_t stream);
 cudaError_t launch_plain(const int32_t *tok, const float *val, const int64_t *off,
