@@ -658,16 +658,19 @@ def evolution_figures(ev, w, torch, sr_stream, generations=5):
             "best_mse": best}
 
 
-def large_figures(ev, rank, flush_buf, sr_stream):
+def large_figures(device, flush_buf, rank):
     """The large population (100,000 expressions of 3-127 tokens, 0-8
     constants, 10 variables, 4M datapoints): forward, fused forward+adjoint
-    and the plain per-expression kernel, one timed launch each after a
-    warm-up launch."""
+    and the plain per-expression kernel.  Its own evaluator, with the
+    untuned default launch shape (timing candidate shapes on launches of
+    seconds would take minutes)."""
     import torch
-    from symbolic_regression_gpu_b200 import _lib
+    from symbolic_regression_gpu_b200 import Evaluator, _lib
     w = make_workload("large", rank)
     pop = w.population
     node_evals = pop.num_tokens * w.num_dps
+    ev = Evaluator(device=device)
+    sr_stream = torch.cuda.ExternalStream(ev.stream_handle, device=torch.device("cuda", device))
     ev.set_data(w.X)
     res = {"workload": "large", "exprs": pop.num_exprs, "num_dps": w.num_dps,
            "num_vars": w.num_vars, "tokens": int(pop.num_tokens)}
@@ -682,6 +685,7 @@ def large_figures(ev, rank, flush_buf, sr_stream):
         res[name] = {"value": node_evals / (ms * 1e-3), "unit": UNIT, "ms": ms}
     res["fwd_adjoint"]["cost_vs_fwd"] = res["fwd_adjoint"]["ms"] / res["fwd"]["ms"]
     res["fwd"]["vs_plain_kernel"] = res["plain_kernel"]["ms"] / res["fwd"]["ms"]
+    ev.close()
     return res
 
 
@@ -820,7 +824,7 @@ def run_ours(args):
         _progress("device evolution figures")
     large = None
     if not args.no_large:
-        large = large_figures(ev, rank, flush_buf, sr_stream)
+        large = large_figures(local_rank, flush_buf, rank)
         _progress("large population figures")
         ev.set_data(w.X)
     plain_config = None
