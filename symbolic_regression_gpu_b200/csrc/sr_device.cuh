@@ -676,7 +676,7 @@ __device__ __forceinline__ void run_program(const Instr *__restrict__ code,
 }
 
 // Sum of the valid squared errors of a lane's DPT datapoints in FP64: the
-// fallback when the FP32 tile sum overflowed (or a square is infinite); exact
+// fallback when the FP32 Kahan sum overflowed (or a square is infinite); exact
 // for DPT finite squares and +Inf when one is infinite, like the reference's
 // double sum.  Out of line: it almost never runs.
 template <int DPT>

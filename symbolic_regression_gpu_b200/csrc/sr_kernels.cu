@@ -15,9 +15,9 @@
 //                             32 lanes x DPT datapoints per instruction fetch,
 //                             accumulator in registers, spilled values in a
 //                             per-warp shared stack.  The epilogue either
-//                             accumulates the squared error (a balanced FP32
-//                             tree over a lane's DPT values, FP64 across tiles
-//                             and lanes) or stores the predictions.
+//                             accumulates the squared error (FP32 Kahan over a
+//                             lane's DPT values, FP64 across tiles and lanes)
+//                             or stores the predictions.
 //  finalize_kernel            per-expression combination of span partials in
 //                             a fixed order: mse = sum / count.
 //  sums_kernel                the same combination kept as (sum, count), for
@@ -124,45 +124,21 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
           float y[DPT];
           lds_vec<DPT>(xs + p.V * span, lane, y);
           const bool full = dp0 + TILE <= p.N;  // warp-uniform
-          // A datapoint counts iff it exists and its prediction is finite
-          // (reference cl_cpu_eval.cpp:147); its squared error is the float
-          // difference squared in float (:149-150).  The lane's DPT squares
-          // are added as a balanced tree; invalid datapoints contribute 0.
-          bool valid[DPT];
-          bool all = true;
+          float s = 0.0f, c = 0.0f;  // Kahan over the lane's DPT values
+          int nv = 0;
 #pragma unroll
           for (int k = 0; k < DPT; ++k) {
-            valid[k] = fabsf(T[k]) <= 3.40282347e38f;
-            all = all && valid[k];
-          }
-          if (!full) {
-#pragma unroll
-            for (int k = 0; k < DPT; ++k) {
-              valid[k] = valid[k] && dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N;
-              all = all && valid[k];
-            }
-          }
-          float sq[DPT];
-          int nv = DPT;
-#pragma unroll
-          for (int k = 0; k < DPT; ++k) {
+            const bool valid =
+                (full || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N) && isfinite(T[k]);
             const float df = __fsub_rn(T[k], y[k]);
-            sq[k] = __fmul_rn(df, df);
+            const float sq = valid ? __fmul_rn(df, df) : 0.0f;
+            nv += valid ? 1 : 0;
+            const float yk = __fsub_rn(sq, c);
+            const float tt = __fadd_rn(s, yk);
+            c = __fsub_rn(__fsub_rn(tt, s), yk);
+            s = tt;
           }
-          if (!all) {
-            nv = 0;
-#pragma unroll
-            for (int k = 0; k < DPT; ++k) {
-              sq[k] = valid[k] ? sq[k] : 0.0f;
-              nv += valid[k] ? 1 : 0;
-            }
-          }
-#pragma unroll
-          for (int n = DPT / 2; n > 0; n /= 2) {
-#pragma unroll
-            for (int k = 0; k < n; ++k) sq[k] = __fadd_rn(sq[k], sq[k + n]);
-          }
-          double tile_sum = static_cast<double>(sq[0]);
+          double tile_sum = static_cast<double>(s) - static_cast<double>(c);
           if (!isfinite(tile_sum)) {
             float tc[DPT], yc[DPT];
 #pragma unroll

@@ -15,7 +15,7 @@ Tolerances (stated once, used below):
     (flagged), and the expressions holding one, are exempt; the exempt shares
     are printed.
   * Reduction error (GPU MSE vs FP64 sum of the GPU's own FP32 predictions):
-    <= oracle.REDUCTION_REL (3e-7) relative, the worst case of the device's
+    <= oracle.REDUCTION_REL (2.5e-7) relative, the worst case of the device's
     summation order.
   * Against the FP64 evaluation: every MSE within max(1e-5, its bound)
     (mode 1 of the same rule: the FP32 evaluation's own rounding).
