@@ -1082,7 +1082,7 @@ static sr_status enqueue_launch(sr_context *ctx, int *launches_out) {
   int launches = 0;
   if (ctx->mode == sr::Mode::kGrad) {
     SR_TRY(launch_grad(ctx));
-    launches = static_cast<int>(ctx->grad.classes.size()) + 1;
+    launches = grad_launch_count(ctx->grad);
   } else if (ctx->mode == sr::Mode::kPlain) {
     SR_TRY_CUDA(ctx, record_event(ctx, 1));
     SR_TRY_CUDA(ctx, sr::launch_plain(ctx->plain.tok.p, ctx->plain.val.p, ctx->plain.off.p,
@@ -1238,8 +1238,10 @@ sr_status sr_read_sums(sr_context *ctx, double *sum_out, double *count_out) {
   SR_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the buffers may grow
   SR_TRY_CUDA(ctx, ctx->sums.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ctx->h_sums.ensure(static_cast<size_t>(E)));
-  if (ctx->mode == sr::Mode::kPlain || ctx->mode == sr::Mode::kGrad)
+  if (ctx->mode == sr::Mode::kPlain)
     SR_TRY_CUDA(ctx, sr::launch_sums(ctx->partial.p, n_spans, E, ctx->sums.p, ctx->stream));
+  else if (ctx->mode == sr::Mode::kGrad)
+    ;  // the gradient finalize kernels wrote ctx->sums
   else
     SR_TRY_CUDA(ctx, sr::launch_finalize_groups(ctx->partial.p, n_spans, E, nullptr,
                                                 ctx->sums.p, ctx->stream));

@@ -27,6 +27,50 @@ namespace capi {
 
 constexpr int kMaxAdjConsts = 64;  // constants per expression with a gradient
 
+// Forward-mode widths (tangent rows per warp): an expression goes to the
+// first launch whose width holds its constants; expressions with more than
+// the widest are differentiated in reverse mode.
+constexpr int kTanWidths[] = {4, sr::kMaxTangentConsts};
+constexpr int kNumTanWidths = 2;
+// Shared memory of a forward-mode block that lets two blocks share an SM.
+constexpr size_t kTanSmemTwoBlocks = 113u * 1024u;
+
+// Mask words of one program for the forward-mode kernel (TanArgs::tmask):
+// the constants (token-order indices, all below kMaxTangentConsts here) under
+// the accumulator before each operator (A) and under its operand b (B), and
+// the constant-load flag.
+void tangent_masks(const Instr *code, int len, uint32_t *out) {
+  uint32_t mT = 0;
+  uint32_t mS[32] = {};
+  for (int i = 0; i < len; ++i) {
+    const Instr &in = code[i];
+    if (sr::instr_spill(in.w)) mS[sr::instr_spill_slot(in.w) & 31u] = mT;
+    uint32_t A = mT, L = 0;
+    if (sr::instr_load(in.w)) {
+      const uint32_t ca = in.c & 0x3FFu;
+      const bool cl = sr::instr_leaf_kind(in.w) == sr::kLeafC && ca < 8u;
+      A = cl ? (1u << ca) : 0u;
+      L = cl ? sr::kTanLoadConst : 0u;
+    }
+    uint32_t B = 0;
+    const uint32_t bk = sr::instr_b_kind(in.w);
+    const uint32_t cb = (in.c >> 10) & 0x3FFu;
+    if (bk == sr::kBC && cb < 8u) B = 1u << cb;
+    if (bk == sr::kBS) B = mS[in.b & 31u];
+    mT = A | B;
+    out[i] = A | (B << 8) | L;
+  }
+}
+
+// Kernel launches of one gradient evaluation (forward-mode launches, reverse
+// classes, finalize kernels).
+int grad_launch_count(const sr::GradSet &g) {
+  int n = 0;
+  for (const sr::TanSet &t : g.tsets) n += (t.plan.items() > 0 ? 1 : 0) + 1;
+  for (const sr::AdjClass &cl : g.classes) n += cl.plan.items() > 0 ? 1 : 0;
+  return n + (g.n_rev > 0 ? 1 : 0);
+}
+
 // Compile, lay out constants, split expressions into tape-length classes and
 // upload everything the adjoint launches need.
 sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute) {
@@ -72,11 +116,31 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
       }
     }
   }
-  // Backward range and Jacobian-tape length of each program: the sweep runs
-  // from the last instruction down to the lowest one holding a constant
-  // (lo); the tape holds d out / d T of [lo, len) and d out / d b of the
-  // instructions in that range whose operand b is a constant or a spilled
-  // subtree.
+  // Forward mode for the expressions with at most kMaxTangentConsts
+  // constants, reverse mode for the others.
+  std::vector<std::vector<int32_t>> tan_members(kNumTanWidths);
+  std::vector<int32_t> rev_members;
+  for (int x = 0; x < E; ++x) {
+    const int nc = ps.n_const[static_cast<size_t>(x)];
+    int k = 0;
+    while (k < kNumTanWidths && nc > kTanWidths[k]) ++k;
+    if (k < kNumTanWidths)
+      tan_members[static_cast<size_t>(k)].push_back(x);
+    else
+      rev_members.push_back(x);
+  }
+  g.n_rev = static_cast<int>(rev_members.size());
+  SR_TRY_CUDA(ctx, g.h_tmask.ensure(static_cast<size_t>(ps.n_instr) + 1));
+  std::memset(g.h_tmask.p, 0, (static_cast<size_t>(ps.n_instr) + 1) * sizeof(uint32_t));
+  for (const auto &mem : tan_members)
+    for (int32_t x : mem)
+      tangent_masks(ps.h_code.p + ps.h_off.p[x], ps.h_len.p[x], g.h_tmask.p + ps.h_off.p[x]);
+
+  // Backward range and Jacobian-tape length of each reverse-mode program:
+  // the sweep runs from the last instruction down to the lowest one holding
+  // a constant (lo); the tape holds d out / d T of [lo, len) and d out / d b
+  // of the instructions in that range whose operand b is a constant or a
+  // spilled subtree.
   SR_TRY_CUDA(ctx, g.h_bwd_lo.ensure(static_cast<size_t>(std::max(E, 1))));
   std::vector<int32_t> tape_need(static_cast<size_t>(E));
   for (int x = 0; x < E; ++x) {
@@ -113,7 +177,7 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
   static const int kTapeClasses[] = {8, 16, 32, 64, 128, 256, 512, 2048};
   constexpr int kNumClasses = 8;
   std::vector<std::vector<int32_t>> members(kNumClasses);
-  for (int x = 0; x < E; ++x) {
+  for (int32_t x : rev_members) {
     const int need = tape_need[static_cast<size_t>(x)];
     int k = 0;
     while (k < kNumClasses - 1 && need > kTapeClasses[k]) ++k;
@@ -205,6 +269,83 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
       table.push_back(q < static_cast<int64_t>(mem.size()) ? mem[static_cast<size_t>(q)] : -1);
     g.classes.push_back(cl);
   }
+  // Forward-mode launches: the interpreter's shape (span groups folded by
+  // each block's producer).
+  g.tsets.clear();
+  std::vector<int32_t> expr_list;
+  int64_t tan_part = 0, tan_gout = 0;
+  for (int k = 0; k < kNumTanWidths; ++k) {
+    auto &mem = tan_members[static_cast<size_t>(k)];
+    if (mem.empty()) continue;
+    sr::TanSet ts;
+    ts.K = 1;
+    for (int32_t x : mem) ts.K = std::max(ts.K, ps.n_const[static_cast<size_t>(x)]);
+    sr::Plan &p = ts.plan;
+    p.dpt = sr::tan_dpt();
+    const int64_t ttile = 32 * p.dpt;
+    p.W = sr::tan_warps();
+    p.smax = ps.smax;
+    p.s_smem = std::min(ps.smax, sr::smem_spill_slots(p.dpt));
+    int64_t tspan = 1024;
+    while (tspan > ttile && 2 * static_cast<int64_t>(ctx->V + 1) * tspan * 4 > 48 * 1024)
+      tspan /= 2;
+    tspan = std::min<int64_t>(tspan, std::max<int64_t>(ttile, round_up(ctx->N, ttile)));
+    // Shorter spans while that lets a second block onto the SM.
+    while (tspan / 2 >= std::max<int64_t>(ttile, 256) && (tspan / 2) % ttile == 0 &&
+           sr::tan_smem_bytes(ts.K, p.W, ctx->V, p.s_smem, static_cast<int>(tspan), p.W * 4) >
+               kTanSmemTwoBlocks)
+      tspan /= 2;
+    // Then fewer evaluating warps while that lets a second block onto the SM.
+    while (p.W > 4 && sr::tan_smem_bytes(ts.K, p.W, ctx->V, p.s_smem, static_cast<int>(tspan),
+                                         p.W * 4) > kTanSmemTwoBlocks)
+      --p.W;
+    p.G = p.W * 4;
+    p.n_groups = static_cast<int>((mem.size() + p.G - 1) / p.G);
+    p.span = static_cast<int>(tspan);
+    p.n_spans = (ctx->N == 0) ? 0 : static_cast<int>((ctx->N + tspan - 1) / tspan);
+    p.smem = sr::tan_smem_bytes(ts.K, p.W, ctx->V, p.s_smem, p.span, p.G);
+    if (p.smem > static_cast<size_t>(dev_max_smem))
+      return ctx->fail(SR_ERR_UNSUPPORTED, "forward-mode launch needs " +
+                                               std::to_string(p.smem) + " bytes of shared memory");
+    p.k_spans = 1;
+    if (p.n_spans > 0) {
+      const int64_t per_sm = static_cast<int64_t>(p.n_spans) * p.n_groups /
+                             (32 * static_cast<int64_t>(std::max(ctx->num_sms, 1)));
+      p.k_spans = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(32, per_sm)));
+    }
+    int bps = 0;
+    SR_TRY_CUDA(ctx, sr::tan_configure(p.smem, p.W, &bps));
+    if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "forward-mode launch does not fit on an SM");
+    p.blocks = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(bps) * ctx->num_sms,
+                                                  std::max<int64_t>(p.items(), 1)));
+    spill_floats = std::max<int64_t>(spill_floats, static_cast<int64_t>(p.blocks) * p.W *
+                                                       (p.smax - p.s_smem) * ttile);
+    std::stable_sort(mem.begin(), mem.end(), [&](int32_t a, int32_t b) {
+      return ps.cost[static_cast<size_t>(a)] > ps.cost[static_cast<size_t>(b)];
+    });
+    ts.group_off = static_cast<int64_t>(table.size());
+    for (int64_t q = 0; q < static_cast<int64_t>(p.n_groups) * p.G; ++q)
+      table.push_back(q < static_cast<int64_t>(mem.size()) ? mem[static_cast<size_t>(q)] : -1);
+    ts.n_exprs = static_cast<int>(mem.size());
+    ts.expr_off = static_cast<int64_t>(expr_list.size());
+    expr_list.insert(expr_list.end(), mem.begin(), mem.end());
+    ts.part_off = tan_part;
+    tan_part += 2 * static_cast<int64_t>(p.n_span_groups()) * E;
+    ts.gout_off = tan_gout;
+    tan_gout += static_cast<int64_t>(p.n_span_groups()) * C;
+    g.tsets.push_back(ts);
+  }
+  g.rev_expr_off = static_cast<int64_t>(expr_list.size());
+  expr_list.insert(expr_list.end(), rev_members.begin(), rev_members.end());
+  {
+    const double need = static_cast<double>(tan_part) * sizeof(double2) +
+                        static_cast<double>(tan_gout) * sizeof(double);
+    if (need > 0.9 * static_cast<double>(ctx->device_memory))
+      return ctx->fail(SR_ERR_UNSUPPORTED,
+                       "forward-mode span sums (" + std::to_string(static_cast<int64_t>(need)) +
+                           " bytes) exceed the device memory; split the population or the "
+                           "datapoints");
+  }
   // Uploads.
   const size_t Cs = static_cast<size_t>(std::max<int64_t>(C, 1));
   SR_TRY_CUDA(ctx, g.h_groups.ensure(std::max<size_t>(table.size(), 1)));
@@ -221,11 +362,26 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
   SR_TRY_CUDA(ctx, g.m.ensure(Cs));
   SR_TRY_CUDA(ctx, g.v.ensure(Cs));
   if (spill_floats > 0) SR_TRY_CUDA(ctx, ctx->spill.ensure(static_cast<size_t>(spill_floats)));
-  SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
-                       std::max<int64_t>(static_cast<int64_t>(g.n_spans) * E, 1))));
+  if (tan_part > 0) SR_TRY_CUDA(ctx, g.tan_partial.ensure(static_cast<size_t>(tan_part)));
+  if (tan_gout > 0) SR_TRY_CUDA(ctx, g.tan_gout.ensure(static_cast<size_t>(tan_gout)));
+  if (g.n_rev > 0)
+    SR_TRY_CUDA(ctx, ctx->partial.ensure(static_cast<size_t>(
+                         std::max<int64_t>(static_cast<int64_t>(g.n_spans) * E, 1))));
+  SR_TRY_CUDA(ctx, g.tmask.ensure(static_cast<size_t>(ps.n_instr) + 1));
+  SR_TRY_CUDA(ctx, g.h_exprs.ensure(std::max<size_t>(expr_list.size(), 1)));
+  if (!expr_list.empty())
+    std::memcpy(g.h_exprs.p, expr_list.data(), expr_list.size() * sizeof(int32_t));
+  SR_TRY_CUDA(ctx, g.exprs.ensure(std::max<size_t>(expr_list.size(), 1)));
+  SR_TRY_CUDA(ctx, ctx->sums.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ctx->mse.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
   cudaStream_t s = ctx->stream;
+  SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.tmask.p, g.h_tmask.p,
+                                   (static_cast<size_t>(ps.n_instr) + 1) * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, s));
+  if (!expr_list.empty())
+    SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.exprs.p, g.h_exprs.p, expr_list.size() * sizeof(int32_t),
+                                     cudaMemcpyHostToDevice, s));
   if (!table.empty())
     SR_TRY_CUDA(ctx, cudaMemcpyAsync(g.groups.p, g.h_groups.p, table.size() * sizeof(int32_t),
                                      cudaMemcpyHostToDevice, s));
@@ -246,13 +402,38 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
   return SR_OK;
 }
 
-// Forward + adjoint of every class, then mse / grad.
+// Forward-mode launches, the reverse-mode classes, then mse / grad (and the
+// FP64 sums the datapoint-sharding reads return).
 sr_status launch_grad(sr_context *ctx) {
   sr::GradSet &g = ctx->grad;
   ProgramSet &ps = ctx->main;
   cudaStream_t s = ctx->stream;
   if (g.C > 0) SR_TRY_CUDA(ctx, cudaMemsetAsync(g.grad_acc.p, 0, g.C * sizeof(double), s));
   SR_TRY_CUDA(ctx, record_event(ctx, 1));
+  for (const sr::TanSet &ts : g.tsets) {
+    if (ts.plan.items() == 0) continue;
+    sr::TanArgs a{};
+    a.e = make_args(ctx, ps, ctx->d_counter);
+    a.e.W = ts.plan.W;
+    a.e.smax = ts.plan.smax;
+    a.e.s_smem = ts.plan.s_smem;
+    a.e.G = ts.plan.G;
+    a.e.n_groups = ts.plan.n_groups;
+    a.e.span = ts.plan.span;
+    a.e.n_spans = ts.plan.n_spans;
+    a.e.span_per_item = ts.plan.k_spans;
+    a.e.group_expr = g.groups.p + ts.group_off;
+    a.e.partial = g.tan_partial.p + ts.part_off;
+    a.tmask = g.tmask.p;
+    a.const_off = g.const_off.p;
+    a.const_cnt = g.const_cnt.p;
+    a.gout = g.tan_gout.p + ts.gout_off;
+    a.C = g.C;
+    a.n_valid = ts.n_exprs;
+    a.K = ts.K;
+    SR_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int32_t), s));
+    SR_TRY_CUDA(ctx, sr::launch_tangent(a, ts.plan.blocks, ts.plan.smem, s));
+  }
   for (const sr::AdjClass &cl : g.classes) {
     if (cl.plan.items() == 0) continue;
     sr::AdjArgs a{};
@@ -277,8 +458,17 @@ sr_status launch_grad(sr_context *ctx) {
     SR_TRY_CUDA(ctx, sr::launch_adjoint(a, g.recompute, cl.plan.blocks, cl.plan.smem, s));
   }
   SR_TRY_CUDA(ctx, record_event(ctx, 2));
-  SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E, g.const_off.p,
-                                            g.const_cnt.p, g.grad_acc.p, ctx->mse.p, g.grad.p, s));
+  for (const sr::TanSet &ts : g.tsets)
+    SR_TRY_CUDA(ctx, sr::launch_tan_finalize(
+                         g.tan_partial.p + ts.part_off, g.tan_gout.p + ts.gout_off,
+                         ts.plan.n_span_groups(), ps.E, g.C, g.exprs.p + ts.expr_off, ts.n_exprs,
+                         g.const_off.p, g.const_cnt.p, ts.K, ctx->mse.p, g.grad.p, g.grad_acc.p,
+                         ctx->sums.p, s));
+  if (g.n_rev > 0)
+    SR_TRY_CUDA(ctx, sr::launch_grad_finalize(ctx->partial.p, g.n_spans, ps.E,
+                                              g.exprs.p + g.rev_expr_off, g.n_rev, g.const_off.p,
+                                              g.const_cnt.p, g.grad_acc.p, ctx->mse.p, g.grad.p,
+                                              ctx->sums.p, s));
   return SR_OK;
 }
 
@@ -345,10 +535,10 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
     SR_TRY_CUDA(ctx, sr::launch_adam(g.C, g.grad.p, g.m.p, g.v.p, g.consts.p, g.const_loc.p,
                                      ctx->main.code.p, step, adam->lr, adam->beta1, adam->beta2,
                                      adam->eps, s));
-    launches += static_cast<int>(g.classes.size()) + 2;
+    launches += grad_launch_count(g) + 1;
   }
   SR_TRY(launch_grad(ctx));  // MSE at the final constants
-  launches += static_cast<int>(g.classes.size()) + 1;
+  launches += grad_launch_count(g);
   SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[3], s));
   ctx->timing_valid = true;
   const int E = pop->num_exprs;

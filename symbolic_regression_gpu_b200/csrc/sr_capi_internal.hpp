@@ -62,6 +62,7 @@ sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, const dou
                            const int64_t *off, int min_size, int min_freq, Detection &out);
 sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute);
 sr_status launch_grad(sr_context *ctx);
+int grad_launch_count(const sr::GradSet &g);
 
 }  // namespace capi
 }  // namespace sr

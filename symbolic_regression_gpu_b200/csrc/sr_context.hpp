@@ -179,6 +179,18 @@ struct DetectBufs {
 };
 
 // Device state of a gradient / constant-optimisation call.
+// A forward-mode (tangent) gradient launch: the expressions with at most K
+// constants (and more than the previous width's).
+struct TanSet {
+  int K = 0;
+  int n_exprs = 0;
+  int64_t group_off = 0;  // into the concatenated group table
+  int64_t expr_off = 0;   // into the expression lists
+  int64_t part_off = 0;   // double2 offset of its MSE sums in tan_partial
+  int64_t gout_off = 0;   // double offset of its gradient sums in tan_gout
+  Plan plan;
+};
+
 struct GradSet {
   DevBuf<int64_t> const_off;
   DevBuf<int32_t> const_cnt;
@@ -197,6 +209,18 @@ struct GradSet {
   PinnedBuf<float> h_consts;
   PinnedBuf<int32_t> h_groups;
   std::vector<AdjClass> classes;
+  // Forward-mode launches, their mask words ([instructions + 1], aligned with
+  // the code) and span-group sums; the expression lists (tangent sets first,
+  // then the reverse-mode expressions) that the finalize kernels walk.
+  std::vector<TanSet> tsets;
+  DevBuf<uint32_t> tmask;
+  PinnedBuf<uint32_t> h_tmask;
+  DevBuf<double2> tan_partial;
+  DevBuf<double> tan_gout;
+  DevBuf<int32_t> exprs;
+  PinnedBuf<int32_t> h_exprs;
+  int64_t rev_expr_off = 0;
+  int n_rev = 0;  // expressions evaluated in reverse mode
   int64_t C = 0;
   int span = 0;
   int n_spans = 0;

@@ -721,12 +721,23 @@ __device__ __forceinline__ void dd_add(double &hi, double &lo, double x) {
 
 // What the producer of an MSE launch folds: the span slots, its accumulators
 // and where a finished item's sums go ([span group][E] entries of two
-// double2: (hi, lo) and (count, 0)).
+// double2: (hi, lo) and (count, 0)).  n_valid: expressions in the launch's
+// group table (groups are padded at their end only).  Gradient launches
+// (K > 0) also fold each expression's constant gradients: K doubles per span
+// slot, added in span order into K doubles per expression, written out to
+// gout[span group][C] at the expression's constant offset.
 struct FoldArgs {
   SpanPart *part;  // [kBufs][G]
   GroupAcc *acc;   // [G]
   double2 *out;
-  int G, E;
+  int G, E, n_valid;
+  int K;
+  const double *gpart;       // [kBufs][G][K]
+  double *gacc;              // [G][K]
+  double *gout;              // [span groups][C]
+  const int64_t *const_off;  // [E]
+  const int32_t *const_cnt;  // [E]
+  int64_t C;
 };
 
 // The producer thread of a block: claims work items from the global counter
@@ -762,6 +773,11 @@ __device__ __noinline__ void run_producer(int n_groups, int n_items, int k_spans
       double2 *o = fa.out + 2 * (static_cast<int64_t>(acc_sg) * fa.E + a.e);
       o[0] = make_double2(a.hi, a.lo);
       o[1] = make_double2(a.cnt, 0.0);
+      if (fa.K > 0) {
+        const int nc = min(fa.const_cnt[a.e], fa.K);
+        double *g = fa.gout + static_cast<int64_t>(acc_sg) * fa.C + fa.const_off[a.e];
+        for (int c = 0; c < nc; ++c) g[c] = fa.gacc[j * fa.K + c];
+      }
     }
     acc_item = -1;
   };
@@ -773,8 +789,9 @@ __device__ __noinline__ void run_producer(int n_groups, int n_items, int k_spans
       acc_item = it;
       acc_sg = k_spans > 1 ? it % ((n_spans + k_spans - 1) / k_spans) : it / n_groups;
       const int g = held_group[b];
-      acc_n = min(fa.G, fa.E - g * fa.G);  // groups are padded at their end only
+      acc_n = min(fa.G, fa.n_valid - g * fa.G);  // groups are padded at their end only
       for (int j = 0; j < acc_n; ++j) fa.acc[j] = GroupAcc{0.0, 0.0, 0.0, 0, 0};
+      for (int j = 0; j < acc_n * fa.K; ++j) fa.gacc[j] = 0.0;
     }
     const SpanPart *q = fa.part + static_cast<size_t>(b) * fa.G;
     for (int j = 0; j < acc_n; ++j) {
@@ -782,6 +799,10 @@ __device__ __noinline__ void run_producer(int n_groups, int n_items, int k_spans
       dd_add(fa.acc[j].hi, fa.acc[j].lo, v.sum);
       fa.acc[j].cnt += static_cast<double>(v.cnt);
       fa.acc[j].e = v.e;
+    }
+    if (fa.K > 0) {
+      const double *gq = fa.gpart + static_cast<size_t>(b) * fa.G * fa.K;
+      for (int j = 0; j < acc_n * fa.K; ++j) fa.gacc[j] += gq[j];
     }
     held[b] = false;
   };

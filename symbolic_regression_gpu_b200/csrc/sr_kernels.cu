@@ -83,7 +83,8 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
     if (lane == 0)
       run_producer<!PRED>(p.n_groups, n_items, k_spans, p.n_spans, p.work_counter, p.error, p.X,
                           p.ldx, rows, span, xbuf, desc, full, empty,
-                          FoldArgs{part, gacc, p.partial, p.G, p.E});
+                          FoldArgs{part, gacc, p.partial, p.G, p.E, p.E, 0, nullptr, nullptr, nullptr,
+                                   nullptr, nullptr, 0});
     return;
   }
 

@@ -278,3 +278,91 @@ def adjoint_bytecode(code, X, V, n_const, n_slots=16, dtype=np.float64, with_abs
     if with_abs:
         return mse, g, (gabs / cnt if cnt else np.full(n_const, np.nan))
     return mse, g
+
+
+# ---- FP32 forward mode (tangents) over the compiled bytecode ----------------
+
+MAX_TANGENT_CONSTS = 8  # expressions with at most this many constants
+
+
+def _kill(d, t, D):
+    """d == 0 ? 0 : d * t, rounded to D."""
+    with np.errstate(all="ignore"):
+        return np.where(d == 0, D(0), (np.asarray(d, D) * np.asarray(t, D)).astype(D)).astype(D)
+
+
+def tangent_bytecode(code, X, V, n_const, n_slots=16, dtype=np.float32, with_abs=False):
+    """MSE and d MSE / d constants of one compiled program, run the way the
+    forward-mode kernel runs it: tangents t_c = d T / d constant c carried
+    beside T; per instruction t_c = dT * t_c for the constants under the
+    accumulator and t_c = db * t_c(b) for the constants under the operand (a
+    zero partial gives zero, whatever the tangent); a constant leaf starts
+    t_c = 1.  Only the constants under a value are carried with it, so a
+    partial never multiplies a constant that is not below it.  Gradients are
+    sum over valid datapoints of (seed == 0 ? 0 : seed * t_c), seed =
+    2 (pred - y), in float64 over the float32 products."""
+    N = X.shape[1]
+    D = dtype
+    y = X[V].astype(D)
+    S = [np.zeros(N, D) for _ in range(n_slots)]
+    ST = [dict() for _ in range(n_slots)]
+    T = np.zeros(N, D)
+    t = {}
+
+    def leaf(kind, payload):
+        if kind == 0:
+            return X[int(payload)].astype(D)
+        return np.full(N, D(np.array([payload], np.uint32).view(F)[0]))
+
+    for i, (w, a, b, c) in enumerate(code):
+        w, c = int(w), int(c)
+        op, bk = w & 63, (w >> 9) & 7
+        if w & (1 << 12):
+            S[(w >> 13) & 31] = T.copy()
+            ST[(w >> 13) & 31] = {k: v.copy() for k, v in t.items()}
+        if w & (1 << 6):
+            lk = (w >> 7) & 3
+            T = leaf(lk, a)
+            ca = c & 0x3FF
+            t = {ca: np.ones(N, D)} if (lk == 1 and ca != 0x3FF) else {}
+        tb = {}
+        if bk == 0:
+            vb = np.zeros(N, D)
+        elif bk == 1:
+            vb = S[int(b)]
+            tb = ST[int(b)]
+        else:
+            vb = leaf(0 if bk == 2 else 1, b)
+            cb = (c >> 10) & 0x3FF
+            if bk == 3 and cb != 0x3FF:
+                tb = {cb: np.ones(N, D)}
+        Tin = T
+        if bk == 0:
+            T = _op64(op, Tin, None)
+            dT, db = _partials64(op, Tin, None, np.asarray(T, D))
+        elif op > 40:
+            T = _op64(op - 40, vb, Tin)
+            db, dT = _partials64(op - 40, vb, Tin, np.asarray(T, D))
+        else:
+            T = _op64(op, Tin, vb)
+            dT, db = _partials64(op, Tin, vb, np.asarray(T, D))
+        T = np.asarray(T, D)
+        new = {k: _kill(dT, v, D) for k, v in t.items()}
+        new.update({k: _kill(db, v, D) for k, v in tb.items()})
+        t = new
+    with np.errstate(all="ignore"):
+        valid = ~np.isnan(T) & ~np.isinf(T.astype(np.float32))
+    cnt = int(valid.sum())
+    d = np.where(valid, T - y, 0.0).astype(D)
+    mse = (d.astype(np.float64) ** 2).sum() / cnt if cnt else np.nan
+    seed = (2.0 * d).astype(D)
+    grad = np.zeros(n_const, np.float64)
+    gabs = np.zeros(n_const, np.float64)
+    for k in range(n_const):
+        g = _kill(seed, t[k], D).astype(np.float64)
+        grad[k] = g.sum()
+        gabs[k] = np.abs(g).sum()
+    g = grad / cnt if cnt else np.full(n_const, np.nan)
+    if with_abs:
+        return mse, g, (gabs / cnt if cnt else np.full(n_const, np.nan))
+    return mse, g

@@ -26,7 +26,7 @@ import numpy as np
 import pytest
 
 import symbolic_regression_gpu_b200 as sg
-from emulate import adjoint_bytecode
+from emulate import MAX_TANGENT_CONSTS, adjoint_bytecode, tangent_bytecode
 from oracle import oracle
 from symbolic_regression_gpu_b200 import _lib
 from symbolic_regression_gpu_b200 import synth
@@ -65,7 +65,9 @@ def _const_expr(pop):
 
 
 def _emulate32(pop, X, V):
-    """(mse [E], grad [C], gabs [C]) of the FP32 bytecode emulator."""
+    """(mse [E], grad [C], gabs [C]) of the FP32 bytecode emulator: forward
+    mode for expressions with at most MAX_TANGENT_CONSTS constants, reverse
+    mode above, as the device evaluates them."""
     code, offs, _ = compile_population(pop, V)
     co = pop.constant_offsets()
     mse = np.empty(pop.num_exprs)
@@ -74,9 +76,10 @@ def _emulate32(pop, X, V):
     with np.errstate(all="ignore"):
         for e in range(pop.num_exprs):
             s = slice(co[e], co[e + 1])
-            mse[e], g[s], ga[s] = adjoint_bytecode(code[offs[e]:offs[e + 1]], X, V,
-                                                   int(co[e + 1] - co[e]), dtype=np.float32,
-                                                   with_abs=True)
+            nc = int(co[e + 1] - co[e])
+            run = tangent_bytecode if nc <= MAX_TANGENT_CONSTS else adjoint_bytecode
+            mse[e], g[s], ga[s] = run(code[offs[e]:offs[e + 1]], X, V, nc, dtype=np.float32,
+                                      with_abs=True)
     return mse, g, ga
 
 
