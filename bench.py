@@ -526,8 +526,12 @@ def _timed_launches(ev, torch, flush_buf, sr_stream, steps):
 
 
 def adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args):
-    """node-evals/s of the forward pass and of the fused forward + adjoint on
-    the constant-optimisation workload, their cost ratio, and 20 Adam steps."""
+    """node-evals/s of the forward pass and of the gradient launches on the
+    constant-optimisation workload, their cost ratio, and 20 Adam steps.
+    "checkpoint" / "recompute" are the library's gradient calls in those modes
+    (forward mode for expressions with at most 8 constants, which is all of
+    this workload); "reverse_checkpoint" / "reverse_recompute" force reverse
+    mode (SR_GRAD_REVERSE_ONLY) for every expression."""
     import torch
     from symbolic_regression_gpu_b200 import _lib
     w = make_workload("grad", rank)
@@ -542,8 +546,12 @@ def adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args):
            "num_vars": w.num_vars, "constants": int(np.count_nonzero(pop.tokens == 0)),
            "fwd": {"value": node_evals / (statistics.mean(fwd_ms) * 1e-3), "unit": UNIT,
                    "ms": statistics.mean(fwd_ms)}}
+    res["forward_mode_exprs"] = int((pop.constant_counts() <= 8).sum())
+    rev = _lib.SR_GRAD_REVERSE_ONLY
     for name, mode in (("checkpoint", _lib.SR_GRAD_CHECKPOINT),
-                       ("recompute", _lib.SR_GRAD_RECOMPUTE)):
+                       ("recompute", _lib.SR_GRAD_RECOMPUTE),
+                       ("reverse_checkpoint", _lib.SR_GRAD_CHECKPOINT | rev),
+                       ("reverse_recompute", _lib.SR_GRAD_RECOMPUTE | rev)):
         try:
             ev.prepare(pop, gradient=True, grad_mode=mode)
         except _lib.SrError as ex:

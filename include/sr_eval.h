@@ -105,6 +105,8 @@ typedef enum sr_status {
 #define SR_EVAL_GRADIENT 0x8u      /* sr_prepare: fused forward + adjoint (MSE and
                                       d MSE / d constants; read with sr_read_grad) */
 #define SR_EVAL_GRAD_RECOMPUTE 0x10u /* with SR_EVAL_GRADIENT: recompute mode      */
+#define SR_EVAL_GRAD_REVERSE 0x20u   /* with SR_EVAL_GRADIENT: reverse mode for every
+                                        expression (see SR_GRAD_REVERSE_ONLY)     */
 
 typedef struct sr_context sr_context;
 
@@ -247,23 +249,32 @@ sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop,
                               int64_t dp_begin, int64_t dp_count,
                               float *pred_out);
 
-/* ---- reverse-mode adjoint (no reference counterpart) ----------------------
+/* ---- gradients with respect to the constants (no reference counterpart) --
  * Constants are the SR_TOK_CONST tokens of each expression, in token order;
  * grad_out uses the same CSR layout as the constants themselves: for
  * expression i its constants are numbered from const_offsets[i], where
  * const_offsets is the exclusive prefix sum of the per-expression constant
  * counts (sr_count_constants).  grad_out[k] = d mse_i / d c_k. */
-/* Both modes run forward and backward fused, per tile of datapoints, in one
- * launch per tape-size class:
+/* Expressions with at most 8 constants are differentiated in forward mode:
+ * one launch runs each program once per tile of datapoints with a tangent per
+ * constant beside every value (no tape, no second pass).  Expressions with
+ * more constants are differentiated in reverse mode, forward and backward
+ * fused per tile, in one launch per tape-size class, with the tape kept as
+ * the mode says:
  *   SR_GRAD_CHECKPOINT keeps every instruction's local partials (the Jacobian
  *     tape) for the tile, in shared memory, or in per-warp global scratch
  *     (L2-resident) when that keeps more warps resident; the backward sweep
  *     reads them.
  *   SR_GRAD_RECOMPUTE keeps only the forward state at segment boundaries and
  *     recomputes each segment's values and partials during the backward sweep
- *     (about one more forward pass, a much smaller tape). */
+ *     (about one more forward pass, a much smaller tape).
+ * SR_GRAD_REVERSE_ONLY, or-ed into the mode, sends every expression through
+ * reverse mode.  Both modes multiply the same local partials along each
+ * constant's path, in opposite orders, so their gradients agree to rounding
+ * (an intermediate product can overflow in one order and not the other). */
 #define SR_GRAD_RECOMPUTE 0
 #define SR_GRAD_CHECKPOINT 1
+#define SR_GRAD_REVERSE_ONLY 2
 sr_status sr_count_constants(const sr_population *pop, int64_t *const_offsets);
 sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode,
                        float *mse_out, float *grad_out, sr_stats *stats);
@@ -280,7 +291,7 @@ sr_status sr_read_grad_sums(sr_context *ctx, double *grad_sum_out);
  * constants (CSR as above), mse_out the MSE at those constants. */
 typedef struct sr_adam_options {
   int32_t steps;
-  int32_t mode; /* SR_GRAD_RECOMPUTE or SR_GRAD_CHECKPOINT */
+  int32_t mode; /* SR_GRAD_RECOMPUTE or SR_GRAD_CHECKPOINT, | SR_GRAD_REVERSE_ONLY */
   float lr, beta1, beta2, eps;
 } sr_adam_options;
 sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,

@@ -37,6 +37,7 @@ SR_EVAL_CLEAR_CACHE = 0x2
 SR_EVAL_PLAIN = 0x4
 SR_EVAL_GRADIENT = 0x8
 SR_EVAL_GRAD_RECOMPUTE = 0x10
+SR_EVAL_GRAD_REVERSE = 0x20
 
 # bounds of sr_eval_mse_device_noalloc (include/sr_eval.h)
 SR_NOALLOC_SCRATCH_BYTES = 4 << 20
@@ -44,6 +45,7 @@ SR_NOALLOC_MAX_EXPRS = (SR_NOALLOC_SCRATCH_BYTES - 256) // 16
 
 SR_GRAD_RECOMPUTE = 0
 SR_GRAD_CHECKPOINT = 1
+SR_GRAD_REVERSE_ONLY = 2
 
 
 class sr_options(Structure):

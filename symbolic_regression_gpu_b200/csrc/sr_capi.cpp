@@ -1053,7 +1053,8 @@ sr_status sr_prepare(sr_context *ctx, const sr_population *pop, uint32_t flags) 
   SR_TRY_CUDA(ctx, ctx->h_mse.ensure(static_cast<size_t>(E)));
   SR_TRY_CUDA(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
   if (flags & SR_EVAL_GRADIENT) {
-    SR_TRY(prepare_grad(ctx, pop, (flags & SR_EVAL_GRAD_RECOMPUTE) != 0));
+    SR_TRY(prepare_grad(ctx, pop, (flags & SR_EVAL_GRAD_RECOMPUTE) != 0,
+                        (flags & SR_EVAL_GRAD_REVERSE) != 0));
     ctx->mode = sr::Mode::kGrad;
   } else if (flags & SR_EVAL_PLAIN) {
     SR_TRY(prepare_plain(ctx, pop));

@@ -73,7 +73,8 @@ int grad_launch_count(const sr::GradSet &g) {
 
 // Compile, lay out constants, split expressions into tape-length classes and
 // upload everything the adjoint launches need.
-sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute) {
+sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute,
+                       bool reverse_only) {
   sr::GradSet &g = ctx->grad;
   g.recompute = recompute;
   ProgramSet &ps = ctx->main;
@@ -117,13 +118,14 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     }
   }
   // Forward mode for the expressions with at most kMaxTangentConsts
-  // constants, reverse mode for the others.
+  // constants, reverse mode for the others (for all with reverse_only).
   std::vector<std::vector<int32_t>> tan_members(kNumTanWidths);
   std::vector<int32_t> rev_members;
   for (int x = 0; x < E; ++x) {
     const int nc = ps.n_const[static_cast<size_t>(x)];
     int k = 0;
     while (k < kNumTanWidths && nc > kTanWidths[k]) ++k;
+    if (reverse_only) k = kNumTanWidths;
     if (k < kNumTanWidths)
       tan_members[static_cast<size_t>(k)].push_back(x);
     else
@@ -291,7 +293,7 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
       tspan /= 2;
     tspan = std::min<int64_t>(tspan, std::max<int64_t>(ttile, round_up(ctx->N, ttile)));
     // Shorter spans while that lets a second block onto the SM.
-    while (tspan / 2 >= std::max<int64_t>(ttile, 256) && (tspan / 2) % ttile == 0 &&
+    while (tspan / 2 >= std::max<int64_t>(ttile, 512) && (tspan / 2) % ttile == 0 &&
            sr::tan_smem_bytes(ts.K, p.W, ctx->V, p.s_smem, static_cast<int>(tspan), p.W * 4) >
                kTanSmemTwoBlocks)
       tspan /= 2;
@@ -482,10 +484,13 @@ sr_status sr_eval_grad(sr_context *ctx, const sr_population *pop, int32_t mode, 
   SR_TRACE("sr_eval_grad");
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
-  if (mode != SR_GRAD_CHECKPOINT && mode != SR_GRAD_RECOMPUTE)
+  const int32_t store = mode & ~SR_GRAD_REVERSE_ONLY;
+  if (store != SR_GRAD_CHECKPOINT && store != SR_GRAD_RECOMPUTE)
     return ctx->fail(SR_ERR_INVALID_ARGUMENT, "unknown gradient mode");
   const double t0 = now_ms();
-  const uint32_t flags = SR_EVAL_GRADIENT | (mode == SR_GRAD_RECOMPUTE ? SR_EVAL_GRAD_RECOMPUTE : 0u);
+  const uint32_t flags = SR_EVAL_GRADIENT |
+                         (store == SR_GRAD_RECOMPUTE ? SR_EVAL_GRAD_RECOMPUTE : 0u) |
+                         ((mode & SR_GRAD_REVERSE_ONLY) ? SR_EVAL_GRAD_REVERSE : 0u);
   SR_TRY(sr_prepare(ctx, pop, flags));
   if (pop->num_exprs == 0) {
     if (stats) *stats = sr_stats{};
@@ -508,7 +513,8 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
   if (!ctx) return SR_ERR_INVALID_ARGUMENT;
   ctx->last_error.clear();
   if (!adam || adam->steps < 0) return ctx->fail(SR_ERR_INVALID_ARGUMENT, "bad Adam options");
-  if (adam->mode != SR_GRAD_CHECKPOINT && adam->mode != SR_GRAD_RECOMPUTE)
+  const int32_t store = adam->mode & ~SR_GRAD_REVERSE_ONLY;
+  if (store != SR_GRAD_CHECKPOINT && store != SR_GRAD_RECOMPUTE)
     return ctx->fail(SR_ERR_INVALID_ARGUMENT, "unknown gradient mode");
   SR_TRY(check_population(ctx, pop));
   if (ctx->V < 0) return ctx->fail(SR_ERR_NO_DATA, "no dataset: call sr_set_data first");
@@ -520,7 +526,8 @@ sr_status sr_optimize_constants(sr_context *ctx, const sr_population *pop,
   reset_prepared(ctx);
   ctx->prep_stats = sr_stats{};
   ctx->E = pop->num_exprs;
-  SR_TRY(prepare_grad(ctx, pop, adam->mode == SR_GRAD_RECOMPUTE));
+  SR_TRY(prepare_grad(ctx, pop, store == SR_GRAD_RECOMPUTE,
+                      (adam->mode & SR_GRAD_REVERSE_ONLY) != 0));
   ctx->mode = sr::Mode::kGrad;
   sr::GradSet &g = ctx->grad;
   cudaStream_t s = ctx->stream;

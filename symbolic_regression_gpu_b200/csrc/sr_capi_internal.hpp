@@ -60,7 +60,8 @@ void fill_stats(sr_context *ctx, sr_stats *st);
 sr_status prepare_plain(sr_context *ctx, const sr_population *pop);
 sr_status detect_on_device(sr_context *ctx, int E, const int32_t *tok, const double *val,
                            const int64_t *off, int min_size, int min_freq, Detection &out);
-sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute);
+sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute,
+                       bool reverse_only);
 sr_status launch_grad(sr_context *ctx);
 int grad_launch_count(const sr::GradSet &g);
 

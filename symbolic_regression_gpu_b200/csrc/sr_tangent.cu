@@ -23,7 +23,8 @@
 //                       instructions with A = B = 0 compute no partials.
 //                       At the end of a tile d MSE / d c gets sum over
 //                       datapoints of seed * t_c, seed = 2 (pred - y) for valid
-//                       datapoints (0 otherwise).  No tape, no second pass.
+//                       datapoints (0 otherwise), summed in FP64.  No tape, no
+//                       second pass.
 //
 // Zero rule (the mirror of the reverse sweep's "a zero adjoint times anything
 // is zero"): a zero partial times anything is zero (t_c = dT == 0 ? 0 :

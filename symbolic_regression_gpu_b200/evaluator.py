@@ -160,13 +160,18 @@ class Evaluator:
                 plain: bool = False, gradient: bool = False,
                 grad_mode: int = _lib.SR_GRAD_CHECKPOINT):
         """Compile and upload `pop` for repeated launch().  gradient=True
-        prepares the fused forward + adjoint (read_mse and read_grad)."""
+        prepares the gradient launches (read_mse and read_grad); grad_mode is
+        SR_GRAD_CHECKPOINT or SR_GRAD_RECOMPUTE, or-ed with
+        SR_GRAD_REVERSE_ONLY to differentiate every expression in reverse
+        mode."""
         cpop = pop.as_c()
         flags = self._flags(cache, clear_cache, plain)
         if gradient:
             flags = _lib.SR_EVAL_GRADIENT
-            if grad_mode == _lib.SR_GRAD_RECOMPUTE:
+            if (grad_mode & ~_lib.SR_GRAD_REVERSE_ONLY) == _lib.SR_GRAD_RECOMPUTE:
                 flags |= _lib.SR_EVAL_GRAD_RECOMPUTE
+            if grad_mode & _lib.SR_GRAD_REVERSE_ONLY:
+                flags |= _lib.SR_EVAL_GRAD_REVERSE
         self._check(_lib.lib.sr_prepare(self._ctx, ctypes.byref(cpop), flags), "sr_prepare")
         self._E = pop.num_exprs
         self._C = int(np.count_nonzero(pop.tokens == 0))

@@ -64,10 +64,11 @@ def _const_expr(pop):
     return np.repeat(np.arange(pop.num_exprs), np.diff(co))
 
 
-def _emulate32(pop, X, V):
+def _emulate32(pop, X, V, reverse_only=False):
     """(mse [E], grad [C], gabs [C]) of the FP32 bytecode emulator: forward
     mode for expressions with at most MAX_TANGENT_CONSTS constants, reverse
-    mode above, as the device evaluates them."""
+    mode above (reverse for all with reverse_only), as the device evaluates
+    them."""
     code, offs, _ = compile_population(pop, V)
     co = pop.constant_offsets()
     mse = np.empty(pop.num_exprs)
@@ -77,13 +78,15 @@ def _emulate32(pop, X, V):
         for e in range(pop.num_exprs):
             s = slice(co[e], co[e + 1])
             nc = int(co[e + 1] - co[e])
-            run = tangent_bytecode if nc <= MAX_TANGENT_CONSTS else adjoint_bytecode
+            forward = nc <= MAX_TANGENT_CONSTS and not reverse_only
+            run = tangent_bytecode if forward else adjoint_bytecode
             mse[e], g[s], ga[s] = run(code[offs[e]:offs[e + 1]], X, V, nc, dtype=np.float32,
                                       with_abs=True)
     return mse, g, ga
 
 
-def test_grad_ieee_ops_match_fp32_emulator(evaluator):
+@pytest.mark.parametrize("reverse_only", [False, True])
+def test_grad_ieee_ops_match_fp32_emulator(evaluator, reverse_only):
     rng = np.random.default_rng(31)
     V, N = 3, 5_000
     X = _dataset(rng, V, N)
@@ -92,8 +95,9 @@ def test_grad_ieee_ops_match_fp32_emulator(evaluator):
     exprs += [gen.sized_tree(int(L)) for L in rng.integers(40, 120, size=20)]
     pop = Population.from_lists(exprs)
     evaluator.set_data(X)
-    mse, g = evaluator.eval_grad(pop)
-    mse_e, g_e, gabs = _emulate32(pop, X, V)
+    mode = _lib.SR_GRAD_CHECKPOINT | (_lib.SR_GRAD_REVERSE_ONLY if reverse_only else 0)
+    mse, g = evaluator.eval_grad(pop, mode=mode)
+    mse_e, g_e, gabs = _emulate32(pop, X, V, reverse_only)
     assert np.array_equal(np.isfinite(g), np.isfinite(g_e))
     fin = np.isfinite(g) & np.isfinite(gabs)
     assert fin.sum() > 300
@@ -262,3 +266,27 @@ def test_recompute_adam(evaluator):
     np.testing.assert_allclose(m_r[fin], m_c[fin], rtol=1e-4)
     seeded = np.arange(0, w.population.num_exprs, 4)
     assert np.median(m_r[seeded] / mse0[seeded]) < 1.0
+
+
+def test_forward_and_reverse_modes_agree(evaluator):
+    """The same population differentiated in forward mode (its expressions
+    have at most 8 constants) and with SR_GRAD_REVERSE_ONLY: the same partials
+    multiplied in opposite orders, so gradients agree to FP32 rounding of the
+    per-datapoint products (1e-5 of the constant's contribution scale gabs)
+    where both are finite, and finiteness differs for under 1% of the
+    constants (an intermediate overflow in one order only)."""
+    w = synth.grad_workload(seed=9, E=300, N=20_000)
+    pop = w.population
+    assert int(pop.constant_counts().max()) <= MAX_TANGENT_CONSTS
+    evaluator.set_data(w.X)
+    mse_f, g_f = evaluator.eval_grad(pop, mode=_lib.SR_GRAD_CHECKPOINT)
+    mse_r, g_r = evaluator.eval_grad(pop, mode=_lib.SR_GRAD_CHECKPOINT | _lib.SR_GRAD_REVERSE_ONLY)
+    fm = np.isfinite(mse_f)
+    assert np.array_equal(fm, np.isfinite(mse_r))
+    assert np.max(_rel(mse_f[fm], mse_r[fm])) <= 1e-6
+    _, _, gabs = _emulate32(pop, w.X, w.num_vars, reverse_only=True)
+    both = np.isfinite(g_f) & np.isfinite(g_r) & np.isfinite(gabs)
+    assert np.mean(np.isfinite(g_f) != np.isfinite(g_r)) <= 0.01
+    assert both.sum() > 500
+    err = _scaled_err(g_f[both], g_r[both].astype(np.float64), gabs[both])
+    assert err.max() <= 1e-5, err.max()
