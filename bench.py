@@ -78,7 +78,9 @@ def parse_args():
     ap.add_argument("--warps", type=int, default=0, help="force evaluating warps per block")
     ap.add_argument("--profile-launch", action="store_true",
                     help="prepare and run a single evaluation, no timing (for ncu)")
-    ap.add_argument("--grad-mode", choices=["none", "checkpoint", "recompute"], default="none",
+    ap.add_argument("--grad-mode", choices=["none", "checkpoint", "recompute",
+                                            "reverse_checkpoint", "reverse_recompute"],
+                    default="none",
                     help="with --profile-launch: run the fused forward + adjoint instead")
     return ap.parse_args()
 
@@ -161,8 +163,10 @@ def profile_launch(args):
         if args.grad_mode == "none":
             ev.prepare(w.population, cache=args.cached, clear_cache=args.cached)
         else:
-            mode = (_lib.SR_GRAD_CHECKPOINT if args.grad_mode == "checkpoint"
+            mode = (_lib.SR_GRAD_CHECKPOINT if args.grad_mode.endswith("checkpoint")
                     else _lib.SR_GRAD_RECOMPUTE)
+            if args.grad_mode.startswith("reverse"):
+                mode |= _lib.SR_GRAD_REVERSE_ONLY
             ev.prepare(w.population, gradient=True, grad_mode=mode)
         ev.launch()
         mse = ev.read_mse()

@@ -435,11 +435,14 @@ static const void *adj_fn(bool global_tape, bool recompute) {
                      : reinterpret_cast<const void *>(&adj_kernel<false, false>);
 }
 
+cudaError_t adj_set_smem_limit(bool global_tape, bool recompute, size_t smem) {
+  return raise_smem_limit(adj_fn(global_tape, recompute), smem);
+}
+
 cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute,
                           int *blocks_per_sm) {
   const void *fn = adj_fn(global_tape, recompute);
-  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+  const cudaError_t err = raise_smem_limit(fn, smem);
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, (W + 1) * 32, smem);
 }
@@ -448,11 +451,6 @@ cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int blocks, size
                            cudaStream_t stream) {
   if (args.e.W < 1 || args.e.W > kMaxWarps) return cudaErrorInvalidValue;
   const void *fn = adj_fn(args.gtape != nullptr, recompute);
-  // Each tape class has its own shared-memory size; the attribute is the
-  // kernel's, so set it for this launch.
-  const cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(smem));
-  if (err != cudaSuccess) return err;
   void *params[] = {const_cast<AdjArgs *>(&args)};
   return cudaLaunchKernel(fn, dim3(blocks), dim3((args.e.W + 1) * 32), params, smem, stream);
 }

@@ -46,6 +46,12 @@ int tan_dpt();    // datapoints per thread
 int tan_warps();  // evaluating warps per block (at most)
 size_t tan_smem_bytes(int K, int W, int V, int s_smem, int span, int G);
 cudaError_t tan_configure(size_t smem, int W, int *blocks_per_sm);
+// The launchers below leave the kernels' maximum dynamic shared memory as it
+// is: a launch sequence raises it first to the largest size any of its
+// launches of that kernel needs (tan_set_smem_limit / adj_set_smem_limit;
+// limits only ever grow, raise_smem_limit), so every launch of a captured
+// sequence is valid on its own.
+cudaError_t tan_set_smem_limit(size_t smem);
 cudaError_t launch_tangent(const TanArgs &args, int blocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_tan_finalize(const double2 *partial, const double *gout, int n_groups, int E,
                                 int64_t C, const int32_t *exprs, int n_exprs,
@@ -61,6 +67,7 @@ size_t adj_smem_bytes(int W, int V, int s_smem, int span, int tape_len, int gmax
 int adj_segment();
 cudaError_t adj_configure(size_t smem, int W, bool global_tape, bool recompute,
                           int *blocks_per_sm);
+cudaError_t adj_set_smem_limit(bool global_tape, bool recompute, size_t smem);
 cudaError_t launch_adjoint(const AdjArgs &args, bool recompute, int blocks, size_t smem,
                            cudaStream_t stream);
 // mse / grad (and the (sum, count) sums) of the n_exprs reverse-mode

@@ -411,6 +411,23 @@ sr_status launch_grad(sr_context *ctx) {
   ProgramSet &ps = ctx->main;
   cudaStream_t s = ctx->stream;
   if (g.C > 0) SR_TRY_CUDA(ctx, cudaMemsetAsync(g.grad_acc.p, 0, g.C * sizeof(double), s));
+  // One shared-memory limit per kernel, the largest its launches here need
+  // (the forward-mode sets share one kernel, and so do the reverse classes
+  // with the same tape placement).
+  {
+    size_t tan_max = 0, adj_max[2] = {0, 0};
+    for (const sr::TanSet &ts : g.tsets)
+      if (ts.plan.items() > 0) tan_max = std::max(tan_max, ts.plan.smem);
+    for (const sr::AdjClass &cl : g.classes)
+      if (cl.plan.items() > 0) {
+        size_t &m = adj_max[cl.global_tape ? 1 : 0];
+        m = std::max(m, cl.plan.smem);
+      }
+    if (tan_max > 0) SR_TRY_CUDA(ctx, sr::tan_set_smem_limit(tan_max));
+    for (int gt = 0; gt < 2; ++gt)
+      if (adj_max[gt] > 0)
+        SR_TRY_CUDA(ctx, sr::adj_set_smem_limit(gt == 1, g.recompute, adj_max[gt]));
+  }
   SR_TRY_CUDA(ctx, record_event(ctx, 1));
   for (const sr::TanSet &ts : g.tsets) {
     if (ts.plan.items() == 0) continue;

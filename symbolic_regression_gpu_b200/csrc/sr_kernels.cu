@@ -507,12 +507,20 @@ static const void *select_interp(int dpt, bool pred, int ops, bool cache, int W)
   return nullptr;
 }
 
+cudaError_t raise_smem_limit(const void *fn, size_t smem) {
+  cudaFuncAttributes a{};
+  const cudaError_t err = cudaFuncGetAttributes(&a, fn);
+  if (err != cudaSuccess) return err;
+  if (static_cast<size_t>(a.maxDynamicSharedSizeBytes) >= smem) return cudaSuccess;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(smem));
+}
+
 cudaError_t interp_configure(int dpt, bool pred, int ops, bool cache, size_t smem, int W,
                              int *blocks_per_sm) {
   const void *fn = select_interp(dpt, pred, ops, cache, W);
   if (!fn || W < 1 || W > kMaxWarps) return cudaErrorInvalidValue;
-  cudaError_t err = cudaFuncSetAttribute(
-      fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  const cudaError_t err = raise_smem_limit(fn, smem);
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn,
                                                        (W + 1) * 32, smem);
@@ -525,8 +533,7 @@ cudaError_t launch_interp(int dpt, bool pred, int ops, bool cache, const EvalArg
   // Plans of one instantiation can differ in shared-memory size (main and
   // cache-fill sets, autotune candidates); the attribute belongs to the
   // kernel, so set it for this launch.
-  const cudaError_t err = cudaFuncSetAttribute(
-      fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  const cudaError_t err = raise_smem_limit(fn, smem);
   if (err != cudaSuccess) return err;
   void *params[] = {const_cast<EvalArgs *>(&args)};
   return cudaLaunchKernel(fn, dim3(blocks), dim3((args.W + 1) * 32), params, smem, stream);

@@ -19,6 +19,11 @@ size_t interp_smem_bytes(int dpt, int W, int V, int s_smem, int span, int G, boo
 // Spill slots per warp kept in shared memory for a datapoints-per-thread
 // choice (deeper slots go to global scratch).
 inline int smem_spill_slots(int dpt) { return dpt >= 16 ? 2 : (dpt == 8 ? 4 : 8); }
+// Raises fn's maximum dynamic shared memory to at least `smem` bytes (never
+// lowers it): a kernel launched by several prepared sequences with different
+// shared-memory sizes keeps a limit that admits every launch already
+// captured, however they are replayed.
+cudaError_t raise_smem_limit(const void *fn, size_t smem);
 // Sets the dynamic-smem attribute and returns resident blocks per SM.
 // `ops` is the operator profile (kOpsAll / kOpsProtected) and `cache` whether
 // the programs read cached subtrees (MSE mode only; prediction launches use

@@ -44,6 +44,7 @@
 #include <stdint.h>
 
 #include "sr_adjoint.hpp"
+#include "sr_kernels.hpp"
 #include "sr_device.cuh"
 #include "sr_grad_ops.cuh"
 
@@ -555,19 +556,17 @@ size_t tan_smem_bytes(int K, int W, int V, int s_smem, int span, int G) {
 cudaError_t tan_configure(size_t smem, int W, int *blocks_per_sm) {
   const void *fn = select_tan();
   if (W < 1 || W > kTanWarps) return cudaErrorInvalidValue;
-  cudaError_t err =
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  const cudaError_t err = raise_smem_limit(fn, smem);
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, (W + 1) * 32, smem);
 }
+
+cudaError_t tan_set_smem_limit(size_t smem) { return raise_smem_limit(select_tan(), smem); }
 
 cudaError_t launch_tangent(const TanArgs &args, int blocks, size_t smem, cudaStream_t stream) {
   const void *fn = select_tan();
   if (args.e.W < 1 || args.e.W > kTanWarps || args.K < 1 || args.K > kMaxTangentConsts)
     return cudaErrorInvalidValue;
-  const cudaError_t err =
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (err != cudaSuccess) return err;
   void *params[] = {const_cast<TanArgs *>(&args)};
   return cudaLaunchKernel(fn, dim3(blocks), dim3((args.e.W + 1) * 32), params, smem, stream);
 }
