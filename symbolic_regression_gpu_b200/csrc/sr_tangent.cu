@@ -23,7 +23,8 @@
 //                       instructions with A = B = 0 compute no partials.
 //                       At the end of a tile d MSE / d c gets sum over
 //                       datapoints of seed * t_c, seed = 2 (pred - y) for valid
-//                       datapoints (0 otherwise), summed in FP64.  No tape, no
+//                       datapoints (0 otherwise): each lane's DPT products in
+//                       FP32, FP64 across lanes, tiles and spans.  No tape, no
 //                       second pass.
 //
 // Zero rule (the mirror of the reverse sweep's "a zero adjoint times anything
@@ -458,15 +459,17 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) tan_kernel(const TanArg
         }
         acc += tile_sum;
         cnt += nv;
-        // d MSE / d c (times the count): seed * t_c, zero where the seed is.
+        // d MSE / d c (times the count): seed * t_c, zero where the seed is;
+        // each lane adds its DPT products in order in FP32, FP64 from there
+        // on (an FP32 lane sum overflows only for products beyond ~4e37).
         for (int cc = 0; cc < nconst; ++cc) {
           float tv[DPT];
           lds_vec<DPT>(tan + cc * TILE, lane, tv);
-          double g = 0.0;
+          float g = sd[0] == 0.0f ? 0.0f : __fmul_rn(sd[0], tv[0]);
 #pragma unroll
-          for (int k = 0; k < DPT; ++k)
-            g += static_cast<double>(sd[k] == 0.0f ? 0.0f : __fmul_rn(sd[k], tv[k]));
-          gl[cc * 32 + lane] += g;
+          for (int k = 1; k < DPT; ++k)
+            g = __fadd_rn(g, sd[k] == 0.0f ? 0.0f : __fmul_rn(sd[k], tv[k]));
+          gl[cc * 32 + lane] += static_cast<double>(g);
         }
       }
 #pragma unroll

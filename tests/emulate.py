@@ -283,6 +283,24 @@ def adjoint_bytecode(code, X, V, n_const, n_slots=16, dtype=np.float64, with_abs
 # ---- FP32 forward mode (tangents) over the compiled bytecode ----------------
 
 MAX_TANGENT_CONSTS = 8  # expressions with at most this many constants
+TANGENT_DPT = 8         # datapoints per thread of the forward-mode kernel
+
+
+def _lane_sums(p, D):
+    """Sum of the products p (length N, rounded to D) the way the forward-mode
+    kernel adds them: tiles of 32 lanes x TANGENT_DPT datapoints (element k of
+    lane l of a tile is datapoint (k // 4) * 128 + 4 l + k % 4), each lane's
+    values added in order in D, then float64 over lanes and tiles."""
+    tile = 32 * TANGENT_DPT
+    n = -(-p.size // tile) * tile
+    q = np.zeros(n, D)
+    q[:p.size] = p
+    q = q.reshape(-1, TANGENT_DPT // 4, 32, 4).transpose(0, 2, 1, 3).reshape(-1, 32, TANGENT_DPT)
+    with np.errstate(all="ignore"):
+        g = q[..., 0].copy()
+        for k in range(1, TANGENT_DPT):
+            g = (g + q[..., k]).astype(D)
+    return g.astype(np.float64).sum()
 
 
 def _kill(d, t, D):
@@ -300,7 +318,7 @@ def tangent_bytecode(code, X, V, n_const, n_slots=16, dtype=np.float32, with_abs
     t_c = 1.  Only the constants under a value are carried with it, so a
     partial never multiplies a constant that is not below it.  Gradients are
     sum over valid datapoints of (seed == 0 ? 0 : seed * t_c), seed =
-    2 (pred - y), in float64 over the float32 products."""
+    2 (pred - y), the products added as the kernel adds them (_lane_sums)."""
     N = X.shape[1]
     D = dtype
     y = X[V].astype(D)
@@ -359,9 +377,9 @@ def tangent_bytecode(code, X, V, n_const, n_slots=16, dtype=np.float32, with_abs
     grad = np.zeros(n_const, np.float64)
     gabs = np.zeros(n_const, np.float64)
     for k in range(n_const):
-        g = _kill(seed, t[k], D).astype(np.float64)
-        grad[k] = g.sum()
-        gabs[k] = np.abs(g).sum()
+        g = _kill(seed, t[k], D)
+        grad[k] = _lane_sums(g, D)
+        gabs[k] = np.abs(g.astype(np.float64)).sum()
     g = grad / cnt if cnt else np.full(n_const, np.nan)
     if with_abs:
         return mse, g, (gabs / cnt if cnt else np.full(n_const, np.nan))
