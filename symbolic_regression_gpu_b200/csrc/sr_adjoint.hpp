@@ -42,16 +42,16 @@ struct TanArgs {
   int32_t K;                  // tangent rows per warp (>= the constants of any expression)
 };
 
-int tan_dpt();    // datapoints per thread
-int tan_warps();  // evaluating warps per block (at most)
+int tan_dpt();         // datapoints per thread
+int tan_warps(int K);  // evaluating warps per block (at most) for K tangent rows
 size_t tan_smem_bytes(int K, int W, int V, int s_smem, int span, int G);
-cudaError_t tan_configure(size_t smem, int W, int *blocks_per_sm);
+cudaError_t tan_configure(int K, size_t smem, int W, int *blocks_per_sm);
 // The launchers below leave the kernels' maximum dynamic shared memory as it
 // is: a launch sequence raises it first to the largest size any of its
 // launches of that kernel needs (tan_set_smem_limit / adj_set_smem_limit;
 // limits only ever grow, raise_smem_limit), so every launch of a captured
 // sequence is valid on its own.
-cudaError_t tan_set_smem_limit(size_t smem);
+cudaError_t tan_set_smem_limit(int K, size_t smem);
 cudaError_t launch_tangent(const TanArgs &args, int blocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_tan_finalize(const double2 *partial, const double *gout, int n_groups, int E,
                                 int64_t C, const int32_t *exprs, int n_exprs,

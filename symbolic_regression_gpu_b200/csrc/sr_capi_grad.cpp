@@ -285,9 +285,11 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     sr::Plan &p = ts.plan;
     p.dpt = sr::tan_dpt();
     const int64_t ttile = 32 * p.dpt;
-    p.W = sr::tan_warps();
+    p.W = sr::tan_warps(ts.K);
     p.smax = ps.smax;
-    p.s_smem = std::min(ps.smax, sr::smem_spill_slots(p.dpt));
+    // Wider sets keep one spill slot per warp in shared memory (the others in
+    // per-warp global scratch): the tangent rows need the room.
+    p.s_smem = std::min(ps.smax, ts.K > 4 ? 1 : sr::smem_spill_slots(p.dpt));
     int64_t tspan = 1024;
     while (tspan > ttile && 2 * static_cast<int64_t>(ctx->V + 1) * tspan * 4 > 48 * 1024)
       tspan /= 2;
@@ -316,7 +318,7 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
       p.k_spans = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(32, per_sm)));
     }
     int bps = 0;
-    SR_TRY_CUDA(ctx, sr::tan_configure(p.smem, p.W, &bps));
+    SR_TRY_CUDA(ctx, sr::tan_configure(ts.K, p.smem, p.W, &bps));
     if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "forward-mode launch does not fit on an SM");
     p.blocks = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(bps) * ctx->num_sms,
                                                   std::max<int64_t>(p.items(), 1)));
@@ -412,18 +414,22 @@ sr_status launch_grad(sr_context *ctx) {
   cudaStream_t s = ctx->stream;
   if (g.C > 0) SR_TRY_CUDA(ctx, cudaMemsetAsync(g.grad_acc.p, 0, g.C * sizeof(double), s));
   // One shared-memory limit per kernel, the largest its launches here need
-  // (the forward-mode sets share one kernel, and so do the reverse classes
-  // with the same tape placement).
+  // (forward-mode sets of the same width class share a kernel, and so do the
+  // reverse classes with the same tape placement).
   {
-    size_t tan_max = 0, adj_max[2] = {0, 0};
+    size_t tan_max[2] = {0, 0}, adj_max[2] = {0, 0};
     for (const sr::TanSet &ts : g.tsets)
-      if (ts.plan.items() > 0) tan_max = std::max(tan_max, ts.plan.smem);
+      if (ts.plan.items() > 0) {
+        size_t &m = tan_max[ts.K > 4 ? 1 : 0];
+        m = std::max(m, ts.plan.smem);
+      }
     for (const sr::AdjClass &cl : g.classes)
       if (cl.plan.items() > 0) {
         size_t &m = adj_max[cl.global_tape ? 1 : 0];
         m = std::max(m, cl.plan.smem);
       }
-    if (tan_max > 0) SR_TRY_CUDA(ctx, sr::tan_set_smem_limit(tan_max));
+    if (tan_max[0] > 0) SR_TRY_CUDA(ctx, sr::tan_set_smem_limit(4, tan_max[0]));
+    if (tan_max[1] > 0) SR_TRY_CUDA(ctx, sr::tan_set_smem_limit(8, tan_max[1]));
     for (int gt = 0; gt < 2; ++gt)
       if (adj_max[gt] > 0)
         SR_TRY_CUDA(ctx, sr::adj_set_smem_limit(gt == 1, g.recompute, adj_max[gt]));

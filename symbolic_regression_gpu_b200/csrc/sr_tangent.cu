@@ -535,16 +535,19 @@ const void *tan_fn() {
   return reinterpret_cast<const void *>(&tan_kernel<DPT, MAXW, MINB>);
 }
 
-// Launch shape: 8 datapoints per thread, at most 8 evaluating warps, at least
-// 2 blocks per SM.
+// Launch shapes: 8 datapoints per thread, at least 2 blocks per SM; at most 8
+// evaluating warps for up to 4 tangent rows, 7 (more registers per thread)
+// for more rows, whose shared memory admits no more warps anyway.
 constexpr int kTanDpt = 8;
-constexpr int kTanWarps = 8;
-const void *select_tan() { return tan_fn<kTanDpt, kTanWarps, 2>(); }
+constexpr int tan_max_warps(int K) { return K <= 4 ? 8 : 7; }
+const void *select_tan(int K) {
+  return K <= 4 ? tan_fn<kTanDpt, 8, 2>() : tan_fn<kTanDpt, 7, 2>();
+}
 
 }  // namespace
 
 int tan_dpt() { return kTanDpt; }
-int tan_warps() { return kTanWarps; }
+int tan_warps(int K) { return tan_max_warps(K); }
 
 size_t tan_smem_bytes(int K, int W, int V, int s_smem, int span, int G) {
   const size_t tile = 32u * static_cast<size_t>(kTanDpt);
@@ -556,20 +559,22 @@ size_t tan_smem_bytes(int K, int W, int V, int s_smem, int span, int G) {
          static_cast<size_t>(G) * K * (kBufs + 1) * sizeof(double);
 }
 
-cudaError_t tan_configure(size_t smem, int W, int *blocks_per_sm) {
-  const void *fn = select_tan();
-  if (W < 1 || W > kTanWarps) return cudaErrorInvalidValue;
+cudaError_t tan_configure(int K, size_t smem, int W, int *blocks_per_sm) {
+  const void *fn = select_tan(K);
+  if (W < 1 || W > tan_max_warps(K)) return cudaErrorInvalidValue;
   const cudaError_t err = raise_smem_limit(fn, smem);
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, (W + 1) * 32, smem);
 }
 
-cudaError_t tan_set_smem_limit(size_t smem) { return raise_smem_limit(select_tan(), smem); }
+cudaError_t tan_set_smem_limit(int K, size_t smem) {
+  return raise_smem_limit(select_tan(K), smem);
+}
 
 cudaError_t launch_tangent(const TanArgs &args, int blocks, size_t smem, cudaStream_t stream) {
-  const void *fn = select_tan();
-  if (args.e.W < 1 || args.e.W > kTanWarps || args.K < 1 || args.K > kMaxTangentConsts)
-    return cudaErrorInvalidValue;
+  if (args.K < 1 || args.K > kMaxTangentConsts) return cudaErrorInvalidValue;
+  const void *fn = select_tan(args.K);
+  if (args.e.W < 1 || args.e.W > tan_max_warps(args.K)) return cudaErrorInvalidValue;
   void *params[] = {const_cast<TanArgs *>(&args)};
   return cudaLaunchKernel(fn, dim3(blocks), dim3((args.e.W + 1) * 32), params, smem, stream);
 }
