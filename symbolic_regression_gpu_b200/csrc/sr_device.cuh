@@ -767,44 +767,47 @@ __device__ __noinline__ void run_producer(int n_groups, int n_items, int k_spans
   const uint32_t row_bytes = static_cast<uint32_t>(span) * sizeof(float);
 
   auto flush = [&]() {
-    if (!FOLD || acc_item < 0) return;
-    for (int j = 0; j < acc_n; ++j) {
-      const GroupAcc a = fa.acc[j];
-      double2 *o = fa.out + 2 * (static_cast<int64_t>(acc_sg) * fa.E + a.e);
-      o[0] = make_double2(a.hi, a.lo);
-      o[1] = make_double2(a.cnt, 0.0);
-      if (fa.K > 0) {
-        const int nc = min(fa.const_cnt[a.e], fa.K);
-        double *g = fa.gout + static_cast<int64_t>(acc_sg) * fa.C + fa.const_off[a.e];
-        for (int c = 0; c < nc; ++c) g[c] = fa.gacc[j * fa.K + c];
+    if constexpr (FOLD) {
+      if (acc_item < 0) return;
+      for (int j = 0; j < acc_n; ++j) {
+        const GroupAcc a = fa.acc[j];
+        double2 *o = fa.out + 2 * (static_cast<int64_t>(acc_sg) * fa.E + a.e);
+        o[0] = make_double2(a.hi, a.lo);
+        o[1] = make_double2(a.cnt, 0.0);
+        if (fa.K > 0) {
+          const int nc = min(fa.const_cnt[a.e], fa.K);
+          double *g = fa.gout + static_cast<int64_t>(acc_sg) * fa.C + fa.const_off[a.e];
+          for (int c = 0; c < nc; ++c) g[c] = fa.gacc[j * fa.K + c];
+        }
       }
+      acc_item = -1;
     }
-    acc_item = -1;
   };
   auto fold = [&](uint32_t b) {
-    if (!FOLD) return;
-    const int it = held_item[b];
-    if (it != acc_item) {
-      flush();
-      acc_item = it;
-      acc_sg = k_spans > 1 ? it % ((n_spans + k_spans - 1) / k_spans) : it / n_groups;
-      const int g = held_group[b];
-      acc_n = min(fa.G, fa.n_valid - g * fa.G);  // groups are padded at their end only
-      for (int j = 0; j < acc_n; ++j) fa.acc[j] = GroupAcc{0.0, 0.0, 0.0, 0, 0};
-      for (int j = 0; j < acc_n * fa.K; ++j) fa.gacc[j] = 0.0;
+    if constexpr (FOLD) {
+      const int it = held_item[b];
+      if (it != acc_item) {
+        flush();
+        acc_item = it;
+        acc_sg = k_spans > 1 ? it % ((n_spans + k_spans - 1) / k_spans) : it / n_groups;
+        const int g = held_group[b];
+        acc_n = min(fa.G, fa.n_valid - g * fa.G);  // groups are padded at their end only
+        for (int j = 0; j < acc_n; ++j) fa.acc[j] = GroupAcc{0.0, 0.0, 0.0, 0, 0};
+        for (int j = 0; j < acc_n * fa.K; ++j) fa.gacc[j] = 0.0;
+      }
+      const SpanPart *q = fa.part + static_cast<size_t>(b) * fa.G;
+      for (int j = 0; j < acc_n; ++j) {
+        const SpanPart v = q[j];
+        dd_add(fa.acc[j].hi, fa.acc[j].lo, v.sum);
+        fa.acc[j].cnt += static_cast<double>(v.cnt);
+        fa.acc[j].e = v.e;
+      }
+      if (fa.K > 0) {
+        const double *gq = fa.gpart + static_cast<size_t>(b) * fa.G * fa.K;
+        for (int j = 0; j < acc_n * fa.K; ++j) fa.gacc[j] += gq[j];
+      }
+      held[b] = false;
     }
-    const SpanPart *q = fa.part + static_cast<size_t>(b) * fa.G;
-    for (int j = 0; j < acc_n; ++j) {
-      const SpanPart v = q[j];
-      dd_add(fa.acc[j].hi, fa.acc[j].lo, v.sum);
-      fa.acc[j].cnt += static_cast<double>(v.cnt);
-      fa.acc[j].e = v.e;
-    }
-    if (fa.K > 0) {
-      const double *gq = fa.gpart + static_cast<size_t>(b) * fa.G * fa.K;
-      for (int j = 0; j < acc_n * fa.K; ++j) fa.gacc[j] += gq[j];
-    }
-    held[b] = false;
   };
   auto drain = [&]() {
     // Let copies already issued land before the block exits.
