@@ -381,10 +381,25 @@ __device__ __forceinline__ void load_operand(uint32_t kind, uint32_t payload, fl
 // One switch case per device opcode: T = op(T, b) (T = op(T) for unary
 // operators) for the DPT datapoints of a lane.  Semantics: sr_ops.cuh.
 #define SR_C_NONE case 0: break;
-#define SR_C_ADD case 1: SR_EACH(T[k] = __fadd_rn(T[k], b[k]))
-#define SR_C_SUB case 2: SR_EACH(T[k] = __fsub_rn(T[k], b[k]))
-#define SR_C_RSUB case 42: SR_EACH(T[k] = __fsub_rn(b[k], T[k]))
-#define SR_C_MUL case 3: SR_EACH(T[k] = __fmul_rn(T[k], b[k]))
+// + - * two datapoints at a time in the paired FP32 instructions of sm_100
+// (add.rn.f32x2, mul.rn.f32x2): each half is the same correctly rounded
+// operation, and a - b is a + (-b) exactly, so results are those of the
+// scalar forms (batched subset 12.91 -> 12.70 ms).
+#define SR_PAIRED(EXPR)                                                        \
+  {                                                                            \
+    _Pragma("unroll") for (int k = 0; k < DPT; k += 2) {                       \
+      const float2 t_ = make_float2(T[k], T[k + 1]);                           \
+      const float2 u_ = make_float2(b[k], b[k + 1]);                           \
+      const float2 r_ = (EXPR);                                                \
+      T[k] = r_.x;                                                             \
+      T[k + 1] = r_.y;                                                         \
+    }                                                                          \
+  }                                                                            \
+  break;
+#define SR_C_ADD case 1: SR_PAIRED(__fadd2_rn(t_, u_))
+#define SR_C_SUB case 2: SR_PAIRED(__fadd2_rn(t_, make_float2(-u_.x, -u_.y)))
+#define SR_C_RSUB case 42: SR_PAIRED(__fadd2_rn(u_, make_float2(-t_.x, -t_.y)))
+#define SR_C_MUL case 3: SR_PAIRED(__fmul2_rn(t_, u_))
 #define SR_C_DIV /* NaN when the divisor is 0 */                              \
   case 4: {                                                                    \
     SR_MAP2(v_div, T, T, b)                                                    \

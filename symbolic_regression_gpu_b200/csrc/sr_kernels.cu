@@ -127,12 +127,20 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) interp_kernel(const Eva
           const bool full = dp0 + TILE <= p.N;  // warp-uniform
           float s = 0.0f, c = 0.0f;  // Kahan over the lane's DPT values
           int nv = 0;
+          float dsq[DPT];  // squared residuals, two datapoints per paired operation
+#pragma unroll
+          for (int k = 0; k < DPT; k += 2) {
+            const float2 df2 =
+                __fadd2_rn(make_float2(T[k], T[k + 1]), make_float2(-y[k], -y[k + 1]));
+            const float2 sq2 = __fmul2_rn(df2, df2);
+            dsq[k] = sq2.x;
+            dsq[k + 1] = sq2.y;
+          }
 #pragma unroll
           for (int k = 0; k < DPT; ++k) {
             const bool valid =
                 (full || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N) && isfinite(T[k]);
-            const float df = __fsub_rn(T[k], y[k]);
-            const float sq = valid ? __fmul_rn(df, df) : 0.0f;
+            const float sq = valid ? dsq[k] : 0.0f;
             nv += valid ? 1 : 0;
             const float yk = __fsub_rn(sq, c);
             const float tt = __fadd_rn(s, yk);

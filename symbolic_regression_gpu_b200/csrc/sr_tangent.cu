@@ -59,7 +59,11 @@ enum : int { kDOne = 0, kDNeg = 1, kDGen = 2 };
 template <int DPT>
 __device__ __forceinline__ void kill_mul(float (&t)[DPT], const float (&d)[DPT]) {
 #pragma unroll
-  for (int k = 0; k < DPT; ++k) t[k] = (d[k] == 0.0f) ? 0.0f : __fmul_rn(d[k], t[k]);
+  for (int k = 0; k < DPT; k += 2) {
+    const float2 r = __fmul2_rn(make_float2(d[k], d[k + 1]), make_float2(t[k], t[k + 1]));
+    t[k] = (d[k] == 0.0f) ? 0.0f : r.x;
+    t[k + 1] = (d[k + 1] == 0.0f) ? 0.0f : r.y;
+  }
 }
 
 // Operators outside the inline set: value and partials through the
@@ -116,30 +120,48 @@ __device__ __forceinline__ void tan_apply(uint32_t op, bool live, float (&T)[DPT
     case 0:
       dk = kDOne;
       break;
+    // + - * in paired FP32 instructions (each half correctly rounded, a - b
+    // as a + (-b)): the forward interpreter's values.
     case 1:
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = __fadd_rn(T[k], b[k]);
+      for (int k = 0; k < DPT; k += 2) {
+        const float2 r = __fadd2_rn(make_float2(T[k], T[k + 1]), make_float2(b[k], b[k + 1]));
+        T[k] = r.x;
+        T[k + 1] = r.y;
+      }
       dk = kDOne;
       bk_ = kDOne;
       break;
     case 2:
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = __fsub_rn(T[k], b[k]);
+      for (int k = 0; k < DPT; k += 2) {
+        const float2 r = __fadd2_rn(make_float2(T[k], T[k + 1]), make_float2(-b[k], -b[k + 1]));
+        T[k] = r.x;
+        T[k + 1] = r.y;
+      }
       dk = kDOne;
       bk_ = kDNeg;
       break;
     case kOpReversed + 2:
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) T[k] = __fsub_rn(b[k], T[k]);
+      for (int k = 0; k < DPT; k += 2) {
+        const float2 r = __fadd2_rn(make_float2(b[k], b[k + 1]), make_float2(-T[k], -T[k + 1]));
+        T[k] = r.x;
+        T[k + 1] = r.y;
+      }
       dk = kDNeg;
       bk_ = kDOne;
       break;
     case 3:
 #pragma unroll
-      for (int k = 0; k < DPT; ++k) {
+      for (int k = 0; k < DPT; k += 2) {
         dT[k] = b[k];
+        dT[k + 1] = b[k + 1];
         db[k] = T[k];
-        T[k] = __fmul_rn(T[k], b[k]);
+        db[k + 1] = T[k + 1];
+        const float2 r = __fmul2_rn(make_float2(T[k], T[k + 1]), make_float2(b[k], b[k + 1]));
+        T[k] = r.x;
+        T[k + 1] = r.y;
       }
       break;
     case 8:  // T / protected(b)
@@ -434,12 +456,22 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) tan_kernel(const TanArg
         const bool full_tile = dp0 + TILE <= p.N;  // warp-uniform
         float s = 0.0f, c = 0.0f;  // Kahan over the lane's DPT values
         int nv = 0;
+        float dfs[DPT], dsq[DPT];
+#pragma unroll
+        for (int k = 0; k < DPT; k += 2) {
+          const float2 df2 = __fadd2_rn(make_float2(T[k], T[k + 1]), make_float2(-y[k], -y[k + 1]));
+          const float2 sq2 = __fmul2_rn(df2, df2);
+          dfs[k] = df2.x;
+          dfs[k + 1] = df2.y;
+          dsq[k] = sq2.x;
+          dsq[k + 1] = sq2.y;
+        }
 #pragma unroll
         for (int k = 0; k < DPT; ++k) {
           const bool valid =
               (full_tile || dp0 + (k / 4) * 128 + lane * 4 + (k % 4) < p.N) && isfinite(T[k]);
-          const float df = __fsub_rn(T[k], y[k]);
-          const float sq = valid ? __fmul_rn(df, df) : 0.0f;
+          const float df = dfs[k];
+          const float sq = valid ? dsq[k] : 0.0f;
           nv += valid ? 1 : 0;
           const float yk = __fsub_rn(sq, c);
           const float tt = __fadd_rn(s, yk);
@@ -465,10 +497,15 @@ __global__ void __launch_bounds__((MAXW + 1) * 32, MINB) tan_kernel(const TanArg
         for (int cc = 0; cc < nconst; ++cc) {
           float tv[DPT];
           lds_vec<DPT>(tan + cc * TILE, lane, tv);
-          float g = sd[0] == 0.0f ? 0.0f : __fmul_rn(sd[0], tv[0]);
 #pragma unroll
-          for (int k = 1; k < DPT; ++k)
-            g = __fadd_rn(g, sd[k] == 0.0f ? 0.0f : __fmul_rn(sd[k], tv[k]));
+          for (int k = 0; k < DPT; k += 2) {
+            const float2 r = __fmul2_rn(make_float2(sd[k], sd[k + 1]), make_float2(tv[k], tv[k + 1]));
+            tv[k] = sd[k] == 0.0f ? 0.0f : r.x;
+            tv[k + 1] = sd[k + 1] == 0.0f ? 0.0f : r.y;
+          }
+          float g = tv[0];
+#pragma unroll
+          for (int k = 1; k < DPT; ++k) g = __fadd_rn(g, tv[k]);
           gl[cc * 32 + lane] += static_cast<double>(g);
         }
       }
