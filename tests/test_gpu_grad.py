@@ -290,3 +290,38 @@ def test_forward_and_reverse_modes_agree(evaluator):
     assert both.sum() > 500
     err = _scaled_err(g_f[both], g_r[both].astype(np.float64), gabs[both])
     assert err.max() <= 1e-5, err.max()
+
+
+def test_forward_mode_long_programs_match_fp32_emulator(evaluator):
+    """Forward mode on long programs (60-127 tokens, deep Sethi-Ullman spills,
+    spill slots beyond the ones kept in shared memory) with at most 8
+    constants, IEEE operators only: the same exactness as the short programs
+    against the FP32 emulator."""
+    rng = np.random.default_rng(44)
+    V, N = 3, 4_000
+    X = _dataset(rng, V, N)
+    gen = synth.TreeGen(rng, V, p_const=0.05, binary=IEEE_BINARY, unary=IEEE_UNARY)
+    full = synth.TreeGen(rng, V, p_const=0.05, binary=IEEE_BINARY, unary=IEEE_UNARY,
+                         p_unary=0.0)
+    exprs = []
+    while len(exprs) < 120:
+        # full binary trees of depth 6 (127 tokens, 6 spill slots) and random shapes
+        e = full.depth_tree(6, full=True) if len(exprs) % 2 else gen.sized_tree(
+            int(rng.integers(60, 128)))
+        if 1 <= sum(1 for tk in e[0] if tk == 0) <= MAX_TANGENT_CONSTS:
+            exprs.append(e)
+    pop = Population.from_lists(exprs)
+    _, _, slots = compile_population(pop, V)
+    assert int(slots.max()) >= 5  # beyond the spill slots kept in shared memory
+    evaluator.set_data(X)
+    mse, g = evaluator.eval_grad(pop)
+    mse_e, g_e, gabs = _emulate32(pop, X, V)
+    assert np.array_equal(np.isfinite(g), np.isfinite(g_e))
+    fin = np.isfinite(g) & np.isfinite(gabs)
+    assert fin.sum() > 200
+    excess = np.abs(g[fin] - g_e[fin]) - 2.0**-24 * np.abs(g_e[fin])
+    err = np.maximum(excess, 0) / np.maximum(gabs[fin], 1e-300)
+    assert err.max() <= 1e-10, err.max()
+    mf = np.isfinite(mse_e)
+    assert np.array_equal(np.isfinite(mse), mf)
+    assert np.max(_rel(mse[mf], mse_e[mf])) <= 1e-6
