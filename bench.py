@@ -563,6 +563,7 @@ def adjoint_figures(ev, rank, world, dev, flush_buf, sr_stream, args):
             continue
         _timed_launches(ev, torch, flush_buf, sr_stream, 2)
         ms = _timed_launches(ev, torch, flush_buf, sr_stream, steps)
+        ev.read_mse()  # refreshes ev.stats (launch count of the gradient call)
         grad = ev.read_grad()
         res[name] = {"value": node_evals / (statistics.mean(ms) * 1e-3), "unit": UNIT,
                      "ms": statistics.mean(ms),
