@@ -260,6 +260,16 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
   SR_TRY_CUDA(ctx, sr::interp_configure(dpt, pred, p.ops, p.cache, p.smem, W, &bps));
   if (bps <= 0) return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
   const int64_t resident = static_cast<int64_t>(bps) * ctx->num_sms;
+  // Few single-span items per resident block (a small population over few
+  // datapoints): shorter spans give more, smaller items and a shorter tail.
+  if (!pred && p.k_spans == 1) {
+    while (p.items() < 16 * resident && p.span / 2 >= std::max<int64_t>(tile, 256) &&
+           (p.span / 2) % tile == 0) {
+      p.span /= 2;
+      p.n_spans = static_cast<int>((ctx->N + p.span - 1) / p.span);
+    }
+    p.smem = sr::interp_smem_bytes(dpt, W, ctx->V, p.s_smem, p.span, p.G, pred);
+  }
   p.blocks = static_cast<int>(std::min<int64_t>(resident, std::max<int64_t>(p.items(), 1)));
   // Global scratch for the spill slots that do not fit in shared memory.
   const size_t spill_floats = static_cast<size_t>(p.blocks) * W *
