@@ -390,7 +390,7 @@ void load_tune_cache(sr_context *ctx) {
       continue;
     int dpt = 0, w = 0, split = -1, per_warp = 4;
     const int n = std::sscanf(line.c_str() + b0, "[%d, %d, %d, %d]", &dpt, &w, &split, &per_warp);
-    if (n >= 2 && (dpt == 4 || dpt == 8 || dpt == 16) && w >= 1 && w <= sr::kMaxWarps &&
+    if (n >= 2 && (dpt == 4 || dpt == 8 || dpt == 16) && w >= 1 && w <= sr::kMaxInterpWarps &&
         split >= -1 && split <= sr::kMaxSpillSlots && per_warp >= 1 && per_warp <= 16)
       ctx->tuned[line.substr(q0 + 1, q1 - q0 - 1)] = {dpt, w, n >= 3 ? split : -1,
                                                        n >= 4 ? per_warp : 4};
@@ -447,7 +447,7 @@ static sr_status time_shape(sr_context *ctx, int dpt, int W, int split, int per_
 // reuse each staged X span more, smaller ones balance better).
 sr_status autotune_main(sr_context *ctx, const std::string &key) {
   SR_TRACE("sr: autotune");
-  static const int kCand[][2] = {{16, 8}, {16, 16}, {8, 8}, {8, 16}, {4, 8}, {4, 16}};
+  static const int kCand[][2] = {{16, 8}, {16, 16}, {8, 8}, {8, 15}, {8, 31}, {4, 8}, {4, 16}};
   float best = 1e30f;
   sr_context::TunedShape win{8, 8, -1, 4};
   for (const auto &c : kCand) {
@@ -499,15 +499,26 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
       SR_TRY(autotune_main(ctx, key));
       it = ctx->tuned.find(key);
     }
-    // Untuned defaults, the shapes the autotuner picks on the evolution
-    // workloads: 8 datapoints x 8 warps for the protected profile; 4 x 16 for
-    // populations over every operator, whose larger dispatch switch fits the
-    // instruction cache better at 4 datapoints (150 -> 82 ms on 4,000
-    // all-operator expressions x 1M datapoints).
+    // Untuned defaults: 8 datapoints x 31 warps (one 1,024-thread block per
+    // SM) for the protected profile, 8 x 8 (3 blocks per SM) where the wide
+    // block's shared memory would not fit even at the shortest span (many
+    // variables); 4 x 16 for populations over every operator, whose larger
+    // dispatch switch fits the instruction cache better at 4 datapoints
+    // (150 -> 82 ms on 4,000 all-operator expressions x 1M datapoints).
     const bool prot = protected_profile(ps);
     const bool have = it != ctx->tuned.end();
+    int wide = 8;
+    if (prot) {
+      int dev_max_smem = 0;
+      cudaDeviceGetAttribute(&dev_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+      const int s_smem = std::min(std::max(ps.smax, 0), sr::smem_spill_slots(8));
+      const int W = sr::kMaxInterpWarps;
+      if (sr::interp_smem_bytes(8, W, ctx->V, s_smem, 32 * 8 * 2, W * per_warp, false) <=
+          static_cast<size_t>(dev_max_smem))
+        wide = W;
+    }
     const int tdpt = have ? it->second.dpt : (prot ? 8 : 4);
-    const int tw = have ? it->second.W : (prot ? 8 : 16);
+    const int tw = have ? it->second.W : (prot ? wide : 16);
     // the tuned split belongs to the tuned shape only
     if (have && (dpt == 0 || dpt == tdpt) && (W == 0 || W == tw)) {
       split = it->second.split;
@@ -615,7 +626,7 @@ sr_status sr_create(const sr_options *opts, sr_context **out) {
   if (opts) o = *opts;
   else sr_options_init(&o);
   if (o.dpt != 0 && o.dpt != 4 && o.dpt != 8 && o.dpt != 16) return SR_ERR_INVALID_ARGUMENT;
-  if (o.warps_per_block < 0 || o.warps_per_block > sr::kMaxWarps) return SR_ERR_INVALID_ARGUMENT;
+  if (o.warps_per_block < 0 || o.warps_per_block > sr::kMaxInterpWarps) return SR_ERR_INVALID_ARGUMENT;
   if (o.smem_spill_slots < -1 || o.smem_spill_slots > sr::kMaxSpillSlots)
     return SR_ERR_INVALID_ARGUMENT;
   if (o.cache_capacity < 0 || o.min_subtree_size < 1 || o.min_subtree_freq < 1)
@@ -1360,7 +1371,8 @@ sr_status sr_eval_predictions(sr_context *ctx, const sr_population *pop, int64_t
   SR_TRY_CUDA(ctx, ctx->main.h_row.ensure(static_cast<size_t>(E)));
   for (int x = 0; x < E; ++x) ctx->main.h_row.p[x] = x;
   int dpt = ctx->opts.dpt ? ctx->opts.dpt : 8;
-  int W = ctx->opts.warps_per_block ? ctx->opts.warps_per_block : sr::kMaxWarps;
+  int W = ctx->opts.warps_per_block ? std::min(ctx->opts.warps_per_block, sr::kMaxWarps)
+                                     : sr::kMaxWarps;
   SR_TRY(plan_set(ctx, ctx->main, true, dpt, W));
   SR_TRY(upload_code(ctx, ctx->main));
   SR_TRY(upload_groups(ctx, ctx->main));

@@ -495,10 +495,15 @@ static const void *interp_mse(int ops, bool cache) {
 }
 
 // Instantiations: W <= 8 uses the narrow variants (more blocks per SM, tighter
-// register budget), larger W the wide ones.  MSE launches come in both
-// operator profiles, with and without cached-subtree operands; prediction
-// launches (cache fills, predictions) in kOpsAll without.
+// register budget), larger W the wide ones (up to 16 warps; at 8 datapoints
+// per thread MSE launches also come as 2 blocks of up to 15 + 1 warps and 1
+// block of up to 31 + 1 warps, both at 64 registers: on the batched
+// population the interpreter is latency-bound, and 30 or 31 evaluating warps
+// per SM beat 24 at 72 registers: 65.2 -> 60.1 and 58.8 ms).  MSE launches
+// come in both operator profiles, with and without cached-subtree operands;
+// prediction launches (cache fills, predictions) in kOpsAll without.
 static const void *select_interp(int dpt, bool pred, int ops, bool cache, int W) {
+  if (W > kMaxWarps && (pred || dpt != 8)) return nullptr;
   const bool narrow = W <= 8;
   if (dpt == 16) {
     if (narrow) return pred ? interp_fn<16, true, 8, 2>() : interp_mse<16, 8, 2>(ops, cache);
@@ -506,7 +511,8 @@ static const void *select_interp(int dpt, bool pred, int ops, bool cache, int W)
   }
   if (dpt == 8) {
     if (narrow) return pred ? interp_fn<8, true, 8, 3>() : interp_mse<8, 8, 3>(ops, cache);
-    return pred ? interp_fn<8, true, 16, 1>() : interp_mse<8, 16, 1>(ops, cache);
+    if (pred) return interp_fn<8, true, 16, 1>();
+    return W <= 15 ? interp_mse<8, 15, 2>(ops, cache) : interp_mse<8, 31, 1>(ops, cache);
   }
   if (dpt == 4) {
     if (narrow) return pred ? interp_fn<4, true, 8, 4>() : interp_mse<4, 8, 4>(ops, cache);
@@ -527,7 +533,7 @@ cudaError_t raise_smem_limit(const void *fn, size_t smem) {
 cudaError_t interp_configure(int dpt, bool pred, int ops, bool cache, size_t smem, int W,
                              int *blocks_per_sm) {
   const void *fn = select_interp(dpt, pred, ops, cache, W);
-  if (!fn || W < 1 || W > kMaxWarps) return cudaErrorInvalidValue;
+  if (!fn || W < 1 || W > kMaxInterpWarps) return cudaErrorInvalidValue;
   const cudaError_t err = raise_smem_limit(fn, smem);
   if (err != cudaSuccess) return err;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn,
@@ -537,7 +543,7 @@ cudaError_t interp_configure(int dpt, bool pred, int ops, bool cache, size_t sme
 cudaError_t launch_interp(int dpt, bool pred, int ops, bool cache, const EvalArgs &args,
                           int blocks, size_t smem, cudaStream_t stream) {
   const void *fn = select_interp(dpt, pred, ops, cache, args.W);
-  if (!fn || args.W < 1 || args.W > kMaxWarps) return cudaErrorInvalidValue;
+  if (!fn || args.W < 1 || args.W > kMaxInterpWarps) return cudaErrorInvalidValue;
   // Plans of one instantiation can differ in shared-memory size (main and
   // cache-fill sets, autotune candidates); the attribute belongs to the
   // kernel, so set it for this launch.

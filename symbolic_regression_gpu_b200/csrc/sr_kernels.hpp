@@ -10,6 +10,9 @@ namespace sr {
 
 constexpr int kMaxWarps = 16;                       // evaluating warps per block
 constexpr int kMaxBlockThreads = (kMaxWarps + 1) * 32;  // + producer warp
+// Evaluating warps per block of an MSE interpreter launch at 8 datapoints per
+// thread: 31 + the producer warp = 1,024 threads, one block per SM.
+constexpr int kMaxInterpWarps = 31;
 constexpr int64_t kDataAlign = 4096;               // X / cache row stride multiple
 constexpr int kPlainStack = 128;                    // plain kernel stack depth
 constexpr int kFp64Stack = 96;                      // FP64 reference kernel stack depth

@@ -212,7 +212,7 @@ def test_mse_vs_fp64_oracle(evaluator):
     _assert_mse_rule(w.population, w.X, mse, m64, "FP32 vs FP64", mode=1, bar=oracle.FP64_BAR)
 
 
-@pytest.mark.parametrize("dpt,warps", [(4, 1), (4, 8), (8, 3), (8, 8)])
+@pytest.mark.parametrize("dpt,warps", [(4, 1), (4, 8), (8, 3), (8, 8), (8, 15), (8, 31)])
 def test_launch_shapes_agree(dpt, warps):
     w = synth.plain_workload(seed=14, E=77, N=3001)
     ref = oracle.mse_f32(w.population, w.X)
@@ -266,7 +266,7 @@ def test_wide_datasets_shrink_span(V):
     X = rng.uniform(-2, 2, size=(V + 1, N)).astype(np.float32)
     gen = synth.TreeGen(rng, V, binary=(op.ADD, op.SUB, op.MUL), unary=(op.NEG, op.ABS))
     pop = Population.from_lists([gen.sized_tree(int(L)) for L in rng.integers(1, 400, 30)])
-    for dpt, warps in [(4, 8), (8, 8), (8, 16)]:
+    for dpt, warps in [(4, 8), (8, 8), (8, 16), (8, 31)]:
         with sg.Evaluator(device=0, dpt=dpt, warps_per_block=warps) as ev:
             ev.set_data(X)
             pred = ev.predictions(pop)
