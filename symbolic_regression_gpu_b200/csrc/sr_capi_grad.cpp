@@ -32,8 +32,6 @@ constexpr int kMaxAdjConsts = 64;  // constants per expression with a gradient
 // the widest are differentiated in reverse mode.
 constexpr int kTanWidths[] = {4, sr::kMaxTangentConsts};
 constexpr int kNumTanWidths = 2;
-// Shared memory of a forward-mode block that lets two blocks share an SM.
-constexpr size_t kTanSmemTwoBlocks = 113u * 1024u;
 
 // Mask words of one program for the forward-mode kernel (TanArgs::tmask):
 // the constants (token-order indices, all below kMaxTangentConsts here) under
@@ -294,14 +292,15 @@ sr_status prepare_grad(sr_context *ctx, const sr_population *pop, bool recompute
     while (tspan > ttile && 2 * static_cast<int64_t>(ctx->V + 1) * tspan * 4 > 48 * 1024)
       tspan /= 2;
     tspan = std::min<int64_t>(tspan, std::max<int64_t>(ttile, round_up(ctx->N, ttile)));
-    // Shorter spans while that lets a second block onto the SM.
+    // One block per SM: shorter spans (down to 512 datapoints) while the
+    // block's shared memory does not fit, then fewer evaluating warps.
+    const size_t budget = static_cast<size_t>(dev_max_smem);
     while (tspan / 2 >= std::max<int64_t>(ttile, 512) && (tspan / 2) % ttile == 0 &&
            sr::tan_smem_bytes(ts.K, p.W, ctx->V, p.s_smem, static_cast<int>(tspan), p.W * 4) >
-               kTanSmemTwoBlocks)
+               budget)
       tspan /= 2;
-    // Then fewer evaluating warps while that lets a second block onto the SM.
     while (p.W > 4 && sr::tan_smem_bytes(ts.K, p.W, ctx->V, p.s_smem, static_cast<int>(tspan),
-                                         p.W * 4) > kTanSmemTwoBlocks)
+                                         p.W * 4) > budget)
       --p.W;
     p.G = p.W * 4;
     p.n_groups = static_cast<int>((mem.size() + p.G - 1) / p.G);

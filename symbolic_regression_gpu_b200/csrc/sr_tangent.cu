@@ -572,13 +572,16 @@ const void *tan_fn() {
   return reinterpret_cast<const void *>(&tan_kernel<DPT, MAXW, MINB>);
 }
 
-// Launch shapes: 8 datapoints per thread, at least 2 blocks per SM; at most 8
-// evaluating warps for up to 4 tangent rows, 7 (more registers per thread)
-// for more rows, whose shared memory admits no more warps anyway.
+// Launch shapes: 8 datapoints per thread, one block per SM with as many
+// evaluating warps as the register file holds beside the producer warp: up
+// to 19 (96 registers per thread) for up to 4 tangent rows, 15 (120) for more.
+// The kernel is latency-bound on dependent chains; one large block keeps
+// more warps resident than two blocks of 8 + 1 or 7 + 1 warps did (16 and 12
+// evaluating warps per SM).
 constexpr int kTanDpt = 8;
-constexpr int tan_max_warps(int K) { return K <= 4 ? 8 : 7; }
+constexpr int tan_max_warps(int K) { return K <= 4 ? 19 : 15; }
 const void *select_tan(int K) {
-  return K <= 4 ? tan_fn<kTanDpt, 8, 2>() : tan_fn<kTanDpt, 7, 2>();
+  return K <= 4 ? tan_fn<kTanDpt, 19, 1>() : tan_fn<kTanDpt, 15, 1>();
 }
 
 }  // namespace
