@@ -235,13 +235,16 @@ sr_status plan_set(sr_context *ctx, ProgramSet &ps, bool pred, int dpt, int W, i
     return ctx->fail(SR_ERR_UNSUPPORTED, "launch shape needs " + std::to_string(p.smem) +
                                              " bytes of shared memory");
   p.n_spans = (ctx->N == 0 || E == 0) ? 0 : static_cast<int>((ctx->N + span - 1) / span);
-  // Spans per work item: as many as keep about 32 items per SM (up to 32
-  // spans), so the per-(span group, expression) entries stay small while the
-  // items still balance over the SMs.  The result does not depend on this
+  // Spans per work item: as many as keep about 32 items of 32 expressions
+  // per SM (up to 32 spans), so the per-(span group, expression) entries stay
+  // small while the items still balance over the SMs; counted in units of 32
+  // expressions, so that larger groups (more warps per block) do not cut the
+  // span range into more span groups.  The result does not depend on this
   // choice (the spans' sums are added as double-doubles).
   p.k_spans = 1;
   if (!pred && p.n_spans > 0) {
-    const int64_t per_sm = static_cast<int64_t>(p.n_spans) * p.n_groups /
+    const int64_t units = (static_cast<int64_t>(E) + 31) / 32;
+    const int64_t per_sm = static_cast<int64_t>(p.n_spans) * units /
                            (32 * static_cast<int64_t>(std::max(ctx->num_sms, 1)));
     p.k_spans = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(32, per_sm)));
   }
