@@ -527,7 +527,7 @@ sr_status prepare_main_shape(sr_context *ctx, bool allow_tune) {
       split = it->second.split;
       per_warp = it->second.per_warp;
     }
-    if (dpt == 0) dpt = tdpt;
+    if (dpt == 0) dpt = W > sr::kMaxWarps ? 8 : tdpt;
     if (W == 0) W = tw;
   }
   if (ctx->opts.smem_spill_slots >= 0) split = ctx->opts.smem_spill_slots;
@@ -630,6 +630,8 @@ sr_status sr_create(const sr_options *opts, sr_context **out) {
   else sr_options_init(&o);
   if (o.dpt != 0 && o.dpt != 4 && o.dpt != 8 && o.dpt != 16) return SR_ERR_INVALID_ARGUMENT;
   if (o.warps_per_block < 0 || o.warps_per_block > sr::kMaxInterpWarps) return SR_ERR_INVALID_ARGUMENT;
+  // More than 16 warps per block exist only at 8 datapoints per thread.
+  if (o.warps_per_block > sr::kMaxWarps && o.dpt != 0 && o.dpt != 8) return SR_ERR_INVALID_ARGUMENT;
   if (o.smem_spill_slots < -1 || o.smem_spill_slots > sr::kMaxSpillSlots)
     return SR_ERR_INVALID_ARGUMENT;
   if (o.cache_capacity < 0 || o.min_subtree_size < 1 || o.min_subtree_freq < 1)

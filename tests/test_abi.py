@@ -65,6 +65,29 @@ def test_create_without_device_reports_status():
     assert ei.value.status == _lib.SR_ERR_NO_DEVICE
 
 
+def test_launch_shape_options_are_checked_before_the_device():
+    """Warps per block: 1..31, above 16 only at 8 datapoints per thread (or a
+    tuned datapoint count, which then becomes 8).  The options are checked
+    before the device is looked up, so this runs without a GPU."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import ctypes
+    from symbolic_regression_gpu_b200 import _lib
+
+    def create(dpt, warps):
+        o = _lib.sr_options()
+        assert _lib.lib.sr_options_init(ctypes.byref(o)) == _lib.SR_OK
+        o.dpt, o.warps_per_block = dpt, warps
+        ctx = ctypes.c_void_p()
+        return _lib.lib.sr_create(ctypes.byref(o), ctypes.byref(ctx))
+
+    for dpt, warps in [(8, 31), (0, 31), (8, 15), (4, 16), (16, 16), (0, 0)]:
+        assert create(dpt, warps) == _lib.SR_ERR_NO_DEVICE, (dpt, warps)
+    for dpt, warps in [(8, 32), (4, 17), (16, 31), (12, 8), (8, -1)]:
+        assert create(dpt, warps) == _lib.SR_ERR_INVALID_ARGUMENT, (dpt, warps)
+
+
 def test_null_arguments_are_rejected():
     from symbolic_regression_gpu_b200 import _lib
     assert _lib.lib.sr_create(None, None) == _lib.SR_ERR_INVALID_ARGUMENT
