@@ -118,9 +118,8 @@ typedef struct sr_options {
   int32_t min_subtree_freq; /* detection min frequency; reference 10 (same line) */
   int32_t dpt;              /* datapoints per thread: 0 = tuned, 4, 8 or 16   */
   int32_t warps_per_block;  /* evaluating warps per block: 0 = tuned, 1..31
-                               (above 16 only for MSE launches at 8
-                               datapoints per thread; predictions use at
-                               most 16)                                     */
+                               (above 16 only with dpt 8, or dpt 0, which
+                               then means 8; predictions use at most 16)   */
   int32_t autotune;         /* 1 = time candidate launch shapes on first use  */
   int32_t use_graphs;       /* 1 = sr_launch captures the prepared launch
                                sequence (memsets, kernels, timing events) in
