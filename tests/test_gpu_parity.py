@@ -277,6 +277,32 @@ def test_wide_datasets_shrink_span(V):
         assert (rel(mse[ok], want[ok]) <= oracle.REDUCTION_REL).all(), (V, dpt, warps)
 
 
+@pytest.mark.parametrize("V,want_warps", [(5, 31), (31, 8)])
+def test_default_launch_shape(V, want_warps):
+    # The untuned shape for the protected profile is one 1,024-thread block
+    # per SM (31 evaluating warps) unless its shared memory does not fit even
+    # at 512-datapoint spans (many variables), then 8 warps at 3 blocks per SM.
+    rng = np.random.default_rng(100 + V)
+    N = 20_000
+    X = rng.uniform(-2, 2, size=(V + 1, N)).astype(np.float32)
+    gen = synth.TreeGen(rng, V, binary=(op.ADD, op.SUB, op.MUL), unary=(op.SIN, op.COS))
+    exprs = [gen.sized_tree(int(L)) for L in rng.integers(3, 64, 300)]
+    exprs += [gen.depth_tree(5, full=True) for _ in range(4)]  # 3 spill slots
+    pop = Population.from_lists(exprs)
+    # With 3 spill slots per warp in shared memory, 31 warps and 32 data rows
+    # need more than 227 KB at 512-datapoint spans.
+    assert sg.evaluator.compile_population(pop, V)[2].max() >= 3
+    with sg.Evaluator(device=0) as ev:
+        ev.set_data(X)
+        mse = ev.eval_mse(pop)
+        assert (ev.stats.dpt, ev.stats.warps_per_block) == (8, want_warps)
+        pred = ev.predictions(pop)
+    want = oracle.mse_of_predictions(pred, X[-1])
+    ok = np.isfinite(want)
+    assert (np.isnan(mse) == np.isnan(want)).all()
+    assert (rel(mse[ok], want[ok]) <= oracle.REDUCTION_REL).all()
+
+
 def test_zero_datapoints_gives_nan(evaluator):
     X = np.zeros((3, 0), np.float32)
     evaluator.set_data(X)
